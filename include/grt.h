@@ -1,0 +1,258 @@
+/*
+ * grt.h -- C ABI of the B200-native GR-ray-tracer per-photon hot path.
+ *
+ * This library replaces the body of the reference's host step loop in
+ * integrate_geodesics (src/geodesic_integrate/integrate_cart_ks.hpp:468-527):
+ *   - the per-step Kokkos::parallel_for over Geodesic_cartesian_kerr_schild
+ *     (integrate_cart_ks.hpp:470-481, functor operator() :230-419),
+ *   - the "Count Terminated Photons" parallel_reduce (:496-503),
+ *   - and, in image mode, the host build_observation_products pass
+ *     (src/radiative_transfer/observation.hpp:31-84) behind write_image_products
+ *     (src/output/write_output.hpp:107-142).
+ *
+ * Ownership: a context owns every device buffer.  Callers pass host pointers
+ * that stay caller-owned; the library copies in and out.  No function throws
+ * across this boundary; each returns a grt_status and grt_last_error() holds a
+ * message.  A context is not re-entrant: use one context per host thread.
+ *
+ * Plain C types only (no CUDA or torch types); compiled for sm_100a.
+ */
+#ifndef GRT_H
+#define GRT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRT_ABI_VERSION 1
+
+typedef enum grt_status {
+    GRT_OK = 0,
+    GRT_EINVAL = 1,     /* invalid argument or configuration value */
+    GRT_ECUDA = 2,      /* a CUDA runtime call failed */
+    GRT_ENOMEM = 3,     /* device allocation failed */
+    GRT_ESTATE = 4,     /* call out of order (e.g. run before upload) */
+    GRT_ETIMEOUT = 5,   /* device work hit its iteration limit and returned */
+    GRT_EIO = 6,        /* file could not be read or written */
+    GRT_ENODEV = 7      /* no usable sm_100 device */
+} grt_status;
+
+/* SimulationMode (src/simulation_options.hpp:11) */
+enum { GRT_MODE_IMAGE = 0, GRT_MODE_DISK = 1 };
+/* IntegratorType (src/utils.hpp:169) */
+enum { GRT_RK4 = 0, GRT_RK45 = 1 };
+/* PhotonGeneratorType (src/radiative_transfer/photon_generation.hpp:12-16) */
+enum { GRT_GEN_BLACKBODY = 0, GRT_GEN_POWER_LAW = 1, GRT_GEN_CUSTOM = 2 };
+/* PhotonPhase (src/utils.hpp:135-141) */
+enum { GRT_PHASE_DISK = 0, GRT_PHASE_IMAGE_BACKWARD = 1, GRT_PHASE_IMAGE_FORWARD = 2,
+       GRT_PHASE_IMAGE_ARRIVED = 3, GRT_PHASE_REJECTED = 4 };
+/* Arithmetic form of the trace kernel. */
+enum { GRT_PREC_FP64 = 0,   /* all-FP64, operation order of the reference (parity form) */
+       GRT_PREC_MIXED = 1   /* FP32 stage/metric arithmetic, FP64 state + controller */ };
+
+/*
+ * Every runtime parameter the reference's step functor and step loop read.
+ * Field meanings and defaults are those of the reference's TOML keys
+ * (src/input/toml_config.hpp:129-278, defaults src/utils.cpp:4-37 and
+ * src/simulation_options.hpp:13-32); grt_params_default() fills them.
+ */
+typedef struct grt_params {
+    int32_t mode;                 /* simulation.mode */
+    int32_t integrator;           /* integration.integrator */
+    int32_t precision;            /* GRT_PREC_* (not a reference key) */
+    int32_t generator;            /* photons.generator */
+    double mass;                  /* black_hole.mass   (M_BH) */
+    double spin;                  /* black_hole.spin   (a_BH) */
+    double r_term_min;            /* termination.r_min (default R_HORIZON) */
+    double r_term_max;            /* termination.r_max (default 1.5*camera.distance) */
+    double atol;                  /* integration.atol */
+    double rtol;                  /* integration.rtol */
+    double min_step_scale;        /* 0.01 (utils.hpp:179) */
+    double max_step_scale;        /* 10.0 (utils.hpp:180) */
+    double safety;                /* 0.9  (utils.hpp:178) */
+    int64_t max_steps;            /* integration.max_steps */
+    double termination_percent;   /* integration.termination_percent */
+    uint64_t output_interval;     /* output.interval: termination is checked on these steps */
+    uint64_t nphotons;            /* global photon count the termination fraction divides by */
+    double initial_step;          /* integration.initial_step (dlambda) */
+    double camera_distance;       /* camera.distance */
+    double camera_theta;          /* camera.theta */
+    double camera_phi;            /* camera.phi */
+    double camera_width;          /* camera.width  (plane_dim1) */
+    double camera_height;         /* camera.height (plane_dim2) */
+    int32_t absorption_enabled;   /* radiative_transfer.absorption_enabled */
+    int32_t emission_enabled;     /* radiative_transfer.emission_enabled */
+    double absorption_coefficient;/* radiative_transfer.absorption_coefficient */
+    double emission_coefficient;  /* radiative_transfer.emission_coefficient */
+    int32_t scattering_enabled;   /* scattering.enabled */
+    int32_t rank;                 /* rank offset added to the scattering seed */
+    double scattering_albedo;     /* scattering.albedo */
+    uint64_t scattering_seed;     /* scattering.seed */
+    double superphoton_count_normalization; /* photons.superphoton_count_normalization */
+    double energy_per_cell_erg;   /* photons.energy_per_cell_erg */
+    double power_law_slope;       /* photons.power_law_slope */
+    double nu_min_hz;             /* photons.nu_min_hz */
+    double nu_max_hz;             /* photons.nu_max_hz */
+    double custom_frequency_hz;   /* photons.custom_frequency_hz */
+    double length_cm_per_code;    /* units.* (photon_generation.hpp:18-38) */
+    double time_s_per_code;
+    double density_g_cm3_per_code;
+    double temperature_k_per_code;
+    double four_velocity_cm_s_per_code;
+    double magnetic_gauss_per_code;
+    uint64_t image_nx;            /* output.image_nx */
+    uint64_t image_ny;            /* output.image_ny */
+    uint64_t spectrum_bins;       /* output.spectrum_bins */
+    double spectrum_min_hz;       /* output.spectrum_min_hz */
+    double spectrum_max_hz;       /* output.spectrum_max_hz */
+} grt_params;
+
+/*
+ * Host structure-of-arrays photon state, one pointer per field of the
+ * reference's struct Photons (src/utils.hpp:40-133).  k0..k3 are the covariant
+ * momentum p_mu.  terminate is one byte per photon (0/1).  Any pointer may be
+ * NULL in grt_download_photons to skip that field.
+ */
+typedef struct grt_photon_soa {
+    uint64_t* id;
+    double* frequency;
+    double* emission_frame_energy;
+    double* x0; double* x1; double* x2; double* x3;
+    double* k0; double* k1; double* k2; double* k3;
+    double* I; double* Q; double* U; double* V;
+    double* dlambda;
+    double* theta_disp;
+    double* phi_disp;
+    uint8_t* terminate;
+    uint8_t* phase;
+} grt_photon_soa;
+
+/* What one grt_run call did. */
+typedef struct grt_run_stats {
+    int64_t steps_done;         /* host-loop steps covered (index of last step + 1) */
+    uint64_t n_terminated;      /* photons with terminate set after the run */
+    uint64_t accepted_steps;    /* ray-steps that advanced a photon */
+    uint64_t rejected_attempts; /* RK45 attempts rejected by the controller */
+    uint64_t photon_calls;      /* functor invocations on live photons */
+    uint64_t launches;          /* trace-kernel launches issued */
+    double trace_ms;            /* device time of the trace launches (CUDA events) */
+    int32_t timed_out;          /* 1 if a launch hit its iteration limit */
+    int32_t pad;
+} grt_run_stats;
+
+/* Image products of write_image_products (write_output.hpp:130-141). */
+typedef struct grt_image_products {
+    double* image_I;              /* [image_ny][image_nx] */
+    double* image_Q;
+    double* image_U;
+    double* image_V;
+    double* spectrum_frequency_hz;/* [spectrum_bins] */
+    double* spectrum_I;           /* [spectrum_bins] */
+    uint64_t* arrived_count;      /* [1] */
+} grt_image_products;
+
+/* Launch shape of the trace kernel (chosen by grt_autotune or set by hand). */
+typedef struct grt_launch_config {
+    int32_t threads_per_block;    /* multiple of 32, <= 1024 */
+    int32_t blocks_per_sm;        /* resident blocks launched per SM */
+    int32_t refill_threshold;     /* idle lanes in a warp before it pulls new photons (1..32) */
+    int32_t photons_per_grab;     /* photons a warp claims per queue access, multiple of 32 is not required */
+} grt_launch_config;
+
+typedef struct grt_ctx grt_ctx;
+
+/* Library / build identification. */
+int32_t grt_abi_version(void);
+const char* grt_build_info(void);
+
+/* Fill p with the reference's compiled-in defaults (src/utils.cpp:4-37). */
+void grt_params_default(grt_params* p);
+
+/*
+ * Parse a reference TOML config (same keys, defaults and validation as
+ * toml_config::load_and_apply_toml_config, src/input/toml_config.hpp:129-278)
+ * into p.  numpy_dir/output_dir/name receive input.numpy_dir, output.directory
+ * and simulation.name (may be NULL).  On error returns GRT_EINVAL/GRT_EIO and
+ * writes the message to err (if err_len > 0).
+ */
+grt_status grt_params_from_toml(const char* path, grt_params* p,
+                                char* numpy_dir, size_t numpy_dir_len,
+                                char* output_dir, size_t output_dir_len,
+                                char* name, size_t name_len,
+                                char* err, size_t err_len);
+
+/* Validate p the way the reference's loader does; GRT_EINVAL on failure. */
+grt_status grt_params_validate(const grt_params* p, char* err, size_t err_len);
+
+/* Create a context on the current CUDA device. */
+grt_status grt_create(const grt_params* p, grt_ctx** out);
+void grt_destroy(grt_ctx* ctx);
+const char* grt_last_error(const grt_ctx* ctx);
+grt_status grt_set_params(grt_ctx* ctx, const grt_params* p);
+
+/* Use the caller's CUDA stream (a cudaStream_t passed as void*); NULL = the context's own. */
+grt_status grt_set_stream(grt_ctx* ctx, void* stream);
+grt_status grt_synchronize(grt_ctx* ctx);
+
+/*
+ * Upload the fluid grid: C-order float64 host arrays of shape
+ * (nr, ntheta, nphi) for r/theta/phi/rho/T and (nr, ntheta, nphi, 4) for
+ * vel/mag, exactly the seven NumPy inputs of load_numpy_field_bundle
+ * (src/input/load_python_arrays.hpp:195-223).  Replaces ScatteringFluidGrid
+ * (src/radiative_transfer/scattering.hpp:22-39).  Passing nr*ntheta*nphi == 0
+ * uploads "no fluid" (fluid_available false, integrate_cart_ks.hpp:436-452).
+ */
+grt_status grt_upload_grid(grt_ctx* ctx, size_t nr, size_t ntheta, size_t nphi,
+                           const double* r, const double* theta, const double* phi,
+                           const double* rho, const double* temperature,
+                           const double* vel4, const double* mag4);
+
+/* Load the seven .npy files of a reference input directory and upload them. */
+grt_status grt_upload_grid_numpy_dir(grt_ctx* ctx, const char* numpy_dir);
+
+/* Copy n photons from host SoA into the context (replaces the Photons views). */
+grt_status grt_upload_photons(grt_ctx* ctx, const grt_photon_soa* soa, size_t n);
+
+/*
+ * Initialise nx*ny image-plane photons on the device, one per pixel centre
+ * u = -W/2 + (ix+1/2) W/nx, v = -H/2 + (iy+1/2) H/ny, photon id = id_offset +
+ * iy*nx + ix.  Same construction as initialize_photons_image
+ * (src/radiative_transfer/initialize_photons.hpp:82-170) with the random
+ * screen draw replaced by the deterministic pixel grid.
+ */
+grt_status grt_init_image_photons(grt_ctx* ctx, uint64_t nx, uint64_t ny, uint64_t id_offset);
+
+/*
+ * Advance the photons: equivalent to the reference's step loop for
+ * step in [0, p.max_steps), stopping after the first output step
+ * (step % output_interval == 0 or the last step) at which the terminated
+ * fraction reaches termination_percent.  stats may be NULL.
+ */
+grt_status grt_run(grt_ctx* ctx, grt_run_stats* stats);
+
+/* Copy the photon state back to host SoA (NULL fields are skipped). */
+grt_status grt_download_photons(grt_ctx* ctx, grt_photon_soa* soa);
+size_t grt_photon_count(const grt_ctx* ctx);
+
+/*
+ * Image products of the ImageArrived photons, accumulated on the device
+ * (build_observation_products, observation.hpp:31-84): every output array is
+ * a caller-owned host buffer sized from p.image_nx/ny/spectrum_bins.
+ */
+grt_status grt_get_image_products(grt_ctx* ctx, grt_image_products* out);
+
+/* Write <output_dir>/<name>_image_products.npz like write_image_products. */
+grt_status grt_write_image_products_npz(grt_ctx* ctx, const char* output_dir, const char* name);
+
+/* Launch shape of the trace kernel. */
+grt_status grt_get_launch_config(const grt_ctx* ctx, grt_launch_config* cfg);
+grt_status grt_set_launch_config(grt_ctx* ctx, const grt_launch_config* cfg);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRT_H */
