@@ -1,0 +1,462 @@
+#!/usr/bin/env python3
+"""Benchmark of the GR-ray-tracer hot path on B200.
+
+Workload (default, the configuration the headline metric is quoted on):
+  C2 -- 256x256 image-mode rays, adaptive RK45 (rtol = atol = 1e-8), Kerr
+  a = 0.94, Fishbone-Moncrief torus on a 128x64x64 (r, theta, phi) grid,
+  camera at 1000 M, inclination 17 deg, absorption and emission on.
+  Synthetic inputs (the torus generator), one ray per pixel centre.
+
+A step = one pass of the hot path over the image: initialise the 65,536
+pixel rays on the device, trace them to termination (grt_run), accumulate the
+image products.  `value` is rays/s of the mixed-precision batched form with
+the grid resident in HBM; the plain FP64 form is timed the same way beside it
+and the Stokes-I error of the mixed image against the FP64 image is reported.
+`e2e` repeats the step through the C ABI with host buffers: the photon SoA is
+uploaded from pinned host memory and the image products are copied back every
+step.  L2 is flushed (a 256 MB device write) before every timed step, outside
+the events.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank traces its own full image (replicas, weak scaling);
+times are CUDA-event times, max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "gr-ray-tracer_b200"))
+
+METRIC = "rays/s & RK steps/s on 1 B200: mixed+batched vs FP64 at ≤1e-5 Stokes-I rel err"
+
+# Algorithmic FP64 operations per unit (add/sub, mul, div, sqrt, pow each 1),
+# pinned by the oracle's op-counting instantiation of the reference source
+# (tests/test_opcount.py): one right-hand side, one RK4 step, one RKF45 attempt.
+OPS_RHS = 243
+OPS_RK4_STEP = 1100
+OPS_RK45_ATTEMPT = 1691
+PHOTON_BYTES = 8 * 18 + 2  # id + 17 float64 fields + terminate + phase
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def algorithmic_flops(stats, integrator):
+    if integrator == 0:
+        return stats["accepted_steps"] * OPS_RK4_STEP
+    attempts = stats["accepted_steps"] + stats["rejected_attempts"]
+    return stats["accepted_steps"] * OPS_RHS + attempts * OPS_RK45_ATTEMPT
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def pinned_photons(n):
+    """Photon SoA whose arrays live in pinned (page-locked) host memory."""
+    import numpy as np
+    import torch
+    from grt.abi import PHOTON_FIELDS, PhotonArrays
+    pa = PhotonArrays(0)
+    pa.n = n
+    keep = []
+    for f in PHOTON_FIELDS:
+        dt = {"id": torch.int64, "terminate": torch.uint8, "phase": torch.uint8}.get(f, torch.float64)
+        t = torch.empty(n, dtype=dt, pin_memory=True)
+        keep.append(t)
+        arr = t.numpy()
+        setattr(pa, f, arr.view(np.uint64) if f == "id" else arr)
+    pa._keep = keep
+    return pa
+
+
+def pinned_products(p):
+    import numpy as np
+    import torch
+    from grt.abi import ProductArrays
+    out = ProductArrays(0, 0, 0)
+    out.nx, out.ny, out.bins = p.image_nx, p.image_ny, p.spectrum_bins
+    keep = []
+
+    def mk(shape, dtype=torch.float64):
+        t = torch.zeros(shape, dtype=dtype, pin_memory=True)
+        keep.append(t)
+        return t.numpy()
+    for f in ("image_I", "image_Q", "image_U", "image_V"):
+        setattr(out, f, mk((p.image_ny, p.image_nx)))
+    out.spectrum_frequency_hz = mk((p.spectrum_bins,))
+    out.spectrum_I = mk((p.spectrum_bins,))
+    out.arrived_count = mk((1,), torch.int64).view(np.uint64)
+    out._keep = keep
+    return out
+
+
+def load_traffic():
+    """DRAM bytes per trace launch from the committed ncu summary, if any."""
+    path = ROOT / "profiles" / "trace_kernel_traffic.json"
+    try:
+        return json.loads(path.read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from grt import abi, autotune, lib, workloads
+
+    world, rank, local = dist_setup(args.gpus)
+    w = workloads.WORKLOADS[args.workload]
+    n_rays = w.pixels * w.pixels
+    grid = w.torus()
+    stream = torch.cuda.Stream()
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    forms = {}
+    wanted = set(args.forms.split(","))
+    for name, prec in (("fp64", abi.PREC_FP64), ("mixed_batched", abi.PREC_MIXED)):
+        if name not in wanted:
+            continue
+        p = w.params()
+        p.precision = prec
+        ctx = lib.Context(p)
+        ctx.set_stream(stream.cuda_stream)
+        ctx.upload_grid(grid)
+        forms[name] = ctx
+
+    def prepare(ctx):
+        ctx.init_image_photons(w.pixels, w.pixels)
+
+    # the batched form picks its launch shape with the autotuner; the FP64
+    # form keeps the library's default shape
+    cfg = None
+    if "mixed_batched" in forms and not args.no_autotune:
+        cfg, _, _ = autotune.tune(forms["mixed_batched"], prepare, w.name, log=None)
+    peak64, peak32 = lib.measure_fma_peaks()
+
+    def one_step(ctx):
+        ctx.init_image_photons(w.pixels, w.pixels)
+        st = ctx.run()
+        prod = ctx.image_products()
+        return st, prod
+
+    results = {}
+    images = {}
+    sampler = ClockSampler(local)
+    with sampler:
+        for name, ctx in forms.items():
+            for _ in range(args.warmup):
+                one_step(ctx)
+            torch.cuda.synchronize()
+            barrier(world)
+            total_ms = 0.0
+            trace_ms = 0.0
+            stats_acc = None
+            launches = 0
+            for _ in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush_buf.zero_()
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+                st, prod = one_step(ctx)
+                ev1.record(stream)
+                ev1.synchronize()
+                total_ms += ev0.elapsed_time(ev1)
+                trace_ms += st["trace_ms"]
+                launches += st["launches"] + 2  # init + trace launches + products
+                stats_acc = st
+            torch.cuda.synchronize()
+            barrier(world)
+            total_ms = max_over_ranks(total_ms, world)
+            images[name] = prod.image_I.copy()
+            results[name] = dict(ms_per_step=total_ms / args.steps, trace_ms_per_launch=trace_ms / args.steps,
+                                 stats=stats_acc, launches=launches,
+                                 rays_per_s=world * n_rays * args.steps / (total_ms * 1e-3),
+                                 rk_steps_per_s=world * stats_acc["accepted_steps"] * args.steps / (total_ms * 1e-3))
+    clocks = sampler.summary()
+
+    stokes_err = per_pixel = None
+    if "fp64" in images and "mixed_batched" in images:
+        ref_img = images["fp64"]
+        diff = images["mixed_batched"] - ref_img
+        nref = float(np.linalg.norm(ref_img))
+        stokes_err = float(np.linalg.norm(diff) / nref) if nref > 0 else float(np.linalg.norm(diff))
+        mask = np.abs(ref_img) > 1e-3 * np.abs(ref_img).max()
+        per_pixel = float(np.max(np.abs(diff[mask]) / np.abs(ref_img[mask]))) if mask.any() else 0.0
+    # headline form: the fastest form whose image meets the 1e-5 Stokes-I bar
+    if "mixed_batched" in results and (stokes_err is None or stokes_err <= 1e-5):
+        head = "mixed_batched"
+    else:
+        head = "fp64"
+    H = results[head]
+
+    # ---- e2e: the C ABI with host buffers (pinned), copies inside the timed region ----
+    ctx = forms[head]
+    host_in = pinned_photons(n_rays)
+    ctx.init_image_photons(w.pixels, w.pixels)
+    ctx.download_photons(host_in)
+    host_out = pinned_products(ctx.params)
+    for _ in range(args.warmup):
+        ctx.upload_photons(host_in)
+        ctx.run()
+        ctx.image_products(host_out)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush_buf.zero_()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        ctx.upload_photons(host_in)
+        ctx.run()
+        ctx.image_products(host_out)
+        ev1.record(stream)
+        ev1.synchronize()
+        e2e_ms += ev0.elapsed_time(ev1)
+    e2e_ms = max_over_ranks(e2e_ms, world)
+    p = ctx.params
+    d2h = 8 * (4 * p.image_nx * p.image_ny + p.spectrum_bins + 1)
+    e2e = {"value": world * n_rays * args.steps / (e2e_ms * 1e-3), "unit": "rays/s",
+           "h2d_bytes_per_step": PHOTON_BYTES * n_rays, "d2h_bytes_per_step": d2h}
+
+    # ---- roofline of the dominant kernel (the headline form's trace kernel) ----
+    flops = algorithmic_flops(H["stats"], w.integrator)
+    achieved = flops / (H["trace_ms_per_launch"] * 1e-3) / 1e12
+    traffic = load_traffic().get(f"{w.name}:{head}")
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                "frac": achieved / peak64, "traffic": traffic,
+                "peak_source": "measured this run: FP64 FMA microbenchmark (grt_measure_fma_peaks)",
+                "fp32_peak_tflops": peak32,
+                "flops_per_launch": flops,
+                "ops_per_unit": {"rhs": OPS_RHS, "rk4_step": OPS_RK4_STEP, "rk45_attempt": OPS_RK45_ATTEMPT}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w)
+
+    for c in forms.values():
+        c.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": H["rays_per_s"],
+            "unit": "rays/s",
+            "rk_steps_per_s": H["rk_steps_per_s"],
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": H["ms_per_step"],
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64" if head == "mixed_batched" else "f64",
+            "data": "synthetic (Fishbone-Moncrief torus generator, deterministic pixel-centre rays)",
+            "config": {"workload": w.name, "pixels": f"{w.pixels}x{w.pixels}",
+                       "grid": "x".join(map(str, w.grid)), "spin": w.spin, "inclination_deg": w.inclination_deg,
+                       "integrator": "rk45" if w.integrator else "rk4", "rtol": w.rtol,
+                       "headline_form": head, "launch": cfg,
+                       "l2": "flushed by a 256 MB device write before every timed step (outside the events)",
+                       "parallelism": f"replicas x{world}"},
+            "forms": {k: {"rays_per_s": v["rays_per_s"], "rk_steps_per_s": v["rk_steps_per_s"],
+                          "ms_per_step": v["ms_per_step"], "trace_ms_per_launch": v["trace_ms_per_launch"],
+                          "accepted_steps": v["stats"]["accepted_steps"],
+                          "rejected_attempts": v["stats"]["rejected_attempts"]} for k, v in results.items()},
+            "speedup_mixed_batched_vs_fp64": (results["mixed_batched"]["rays_per_s"] / results["fp64"]["rays_per_s"]
+                                              if len(results) == 2 else None),
+            "stokes_I_rel_err": stokes_err,
+            "stokes_I_max_pixel_rel_err": per_pixel,
+            "e2e": e2e,
+            "gpu_launches": H["launches"],
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(w, reps=2):
+    """The reference's own integrate_geodesics (shim-compiled, oracle/_ref) on
+    the host cores, on the full workload; falls back to the oracle port."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    from grt import config, torus
+    p = w.params()
+    n = w.pixels * w.pixels
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        torus.write_numpy_dir(w.torus(), d / "np")
+        toml = config.write_toml(p, d / "c.toml", d / "np", d / "out")
+        best = None
+        if pyoracle.Reference.available():
+            ref = pyoracle.Reference()
+            kind = "reference"
+            for _ in range(reps):
+                ph = ref.init_image_photons(toml, w.pixels, w.pixels)
+                _, st = ref.run(toml, ph, None)
+                if best is None or st["elapsed_s"] < best[0]:
+                    best = (st["elapsed_s"], st["stepped"])
+        else:
+            o = pyoracle.Oracle()
+            o.set_pow_mode("libm")
+            kind = "port"
+            for _ in range(reps):
+                ph = o.init_image_photons(p, w.pixels, w.pixels)
+                t0 = time.perf_counter()
+                st = o.run(p, w.torus(), ph)
+                dt = time.perf_counter() - t0
+                if best is None or dt < best[0]:
+                    best = (dt, st["accepted_steps"])
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return {"value": n / best[0], "unit": "rays/s", "rk_steps_per_s": best[1] / best[0], "cores": cores,
+            "kind": kind,
+            "sample": f"full {w.name} workload ({n} rays), best of {reps}; reference Kokkos functor via the "
+                      "project OpenMP shim (real Kokkos is not installable offline), OMP threads = all cores"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from grt import workloads
+    w = workloads.WORKLOADS[args.workload]
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(w, reps=1)
+    t_total = 0.0
+    steps_total = 0.0
+    for _ in range(args.steps):
+        c = cpu_baseline(w, reps=1)
+        vals.append(c)
+        t_total += (w.pixels * w.pixels) / c["value"]
+        steps_total += c["rk_steps_per_s"] * (w.pixels * w.pixels) / c["value"]
+    n = w.pixels * w.pixels * args.steps
+    value = n / t_total
+    c = vals[-1]
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rays/s",
+        "rk_steps_per_s": steps_total / t_total, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "pixels": f"{w.pixels}x{w.pixels}", "grid": "x".join(map(str, w.grid))},
+        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": c["cores"], "kind": c["kind"],
+                         "sample": c["sample"]},
+        "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="use the library's default launch shape")
+    ap.add_argument("--forms", default="fp64,mixed_batched", help="comma list of fp64, mixed_batched")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,710 @@
+// C ABI of the hot path (include/grt.h): context, device buffers, the host
+// step loop with the reference's termination semantics, and image products.
+//
+// Reference interfaces replaced (file:line within the reference project):
+//   grt_upload_grid        ScatteringFluidGrid build (integrate_cart_ks.hpp:436-459)
+//   grt_upload_photons     Photons device views (utils.hpp:40-133)
+//   grt_init_image_photons initialize_photons_image (initialize_photons.hpp:82-170)
+//   grt_run                integrate_geodesics step loop (integrate_cart_ks.hpp:468-527)
+//   grt_get_image_products build_observation_products (observation.hpp:31-84)
+//   grt_write_image_products_npz write_image_products (write_output.hpp:107-142)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <string>
+#include <vector>
+
+#include "grt.h"
+#include "grt_host.h"
+#include "grt_kparams.h"
+#include "grt_launch.h"
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+template <class T>
+struct DevBuf {
+    T* ptr = nullptr;
+    size_t count = 0;
+    cudaError_t alloc(size_t n) {
+        if (n <= count && ptr) return cudaSuccess;
+        release();
+        if (n == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T));
+        if (e == cudaSuccess) count = n;
+        else ptr = nullptr;
+        return e;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+};
+
+struct PhotonBufs {
+    DevBuf<uint64_t> id;
+    DevBuf<double> f[17];  // frequency .. phi_disp in grt_photon_soa order
+    DevBuf<uint8_t> term, phase;
+    cudaError_t alloc(size_t n) {
+        cudaError_t e = id.alloc(n);
+        for (auto& b : f)
+            if (e == cudaSuccess) e = b.alloc(n);
+        if (e == cudaSuccess) e = term.alloc(n);
+        if (e == cudaSuccess) e = phase.alloc(n);
+        return e;
+    }
+    void release() {
+        id.release();
+        for (auto& b : f) b.release();
+        term.release();
+        phase.release();
+    }
+    grt::KPhotons view() const {
+        grt::KPhotons k;
+        k.id = id.ptr;
+        double** d[17] = {&k.frequency, &k.emission_frame_energy, &k.x0, &k.x1, &k.x2, &k.x3,
+                          &k.k0, &k.k1, &k.k2, &k.k3, &k.I, &k.Q, &k.U, &k.V,
+                          &k.dlambda, &k.theta_disp, &k.phi_disp};
+        for (int q = 0; q < 17; ++q) *d[q] = f[q].ptr;
+        k.terminate = term.ptr;
+        k.phase = phase.ptr;
+        return k;
+    }
+};
+
+double* const* soa_doubles(const grt_photon_soa* s, double* out[17]) {
+    double* src[17] = {s->frequency, s->emission_frame_energy, s->x0, s->x1, s->x2, s->x3,
+                       s->k0, s->k1, s->k2, s->k3, s->I, s->Q, s->U, s->V,
+                       s->dlambda, s->theta_disp, s->phi_disp};
+    for (int q = 0; q < 17; ++q) out[q] = src[q];
+    return out;
+}
+
+}  // namespace
+
+struct grt_ctx {
+    grt_params p;
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // grid
+    bool grid_uploaded = false;
+    bool fluid_available = false;
+    bool separable = false;
+    int nr = 0, nth = 0, nph = 0;
+    double r_reject_lo = 0.0, r_reject_hi = 0.0;
+    DevBuf<double> r_axis, th_axis, ph_axis, r3, th3, ph3;
+    DevBuf<double2> rho_t, vel, mag;
+    // photons
+    size_t n = 0;
+    PhotonBufs ph;
+    unsigned long long initial_terminated = 0;
+    // scratch: launch counters and products
+    DevBuf<grt::KCounters> counters;
+    grt::KCounters* host_counters = nullptr;  // pinned
+    DevBuf<double> image, spectrum;
+    DevBuf<unsigned long long> arrived;
+    DevBuf<unsigned long long> scratch_u64;
+    unsigned long long* host_u64 = nullptr;  // pinned
+    grt_launch_config lc{256, 1, 8, 32};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+grt_status fail(grt_ctx* c, grt_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+grt_status cuda_fail(grt_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, e == cudaErrorMemoryAllocation ? GRT_ENOMEM : GRT_ECUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define GRT_CUDA(ctx, call, what)                        \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+    } while (0)
+
+// fluid_frame.hpp:28-48 on the host (glibc sin/cos, exactly the reference's
+// arithmetic), then the [units] scale, as sample_scattering_fluid applies it
+// per step (scattering.hpp:223-241).
+void spherical_to_cartesian_vec(double r, double th, double ph, double spin, const double s[4], double scale,
+                                double c[4]) {
+    const double st = std::sin(th), ct = std::cos(th);
+    const double sp = std::sin(ph), cp = std::cos(ph);
+    const double radial_x = cp * st, radial_y = sp * st, radial_z = ct;
+    const double theta_x = (r * cp - spin * sp) * ct;
+    const double theta_y = (r * sp + spin * cp) * ct;
+    const double theta_z = -r * st;
+    const double phi_x = (-r * sp - spin * cp) * st;
+    const double phi_y = (r * cp - spin * sp) * st;
+    c[0] = s[0];
+    c[1] = radial_x * s[1] + theta_x * s[2] + phi_x * s[3];
+    c[2] = radial_y * s[1] + theta_y * s[2] + phi_y * s[3];
+    c[3] = radial_z * s[1] + theta_z * s[2];
+    for (int q = 0; q < 4; ++q) c[q] *= scale;
+}
+
+bool well_separated_increasing(const std::vector<double>& a) {
+    for (size_t i = 1; i < a.size(); ++i) {
+        if (!(a[i] > a[i - 1])) return false;
+        const double gap = a[i] - a[i - 1];
+        const double mag = std::max(std::fabs(a[i]), std::fabs(a[i - 1]));
+        if (!(gap > 1e-12 * mag)) return false;
+    }
+    return true;
+}
+
+grt::KParams make_kparams(const grt_ctx* c) {
+    const grt_params& p = c->p;
+    grt::KParams k;
+    std::memset(&k, 0, sizeof(k));
+    k.a = p.spin;
+    k.M = p.mass;
+    k.r_min = p.r_term_min;
+    k.r_max = p.r_term_max;
+    k.atol = p.atol;
+    k.rtol = p.rtol;
+    k.min_scale = p.min_step_scale;
+    k.max_scale = p.max_step_scale;
+    k.safety = p.safety;
+    k.kappa = p.absorption_coefficient;
+    k.jcoef = p.emission_coefficient;
+    k.albedo = p.scattering_albedo;
+    k.length_scale = p.length_cm_per_code;
+    k.time_scale = p.time_s_per_code;
+    k.density_scale = p.density_g_cm3_per_code;
+    k.temperature_scale = p.temperature_k_per_code;
+    k.norm = p.superphoton_count_normalization;
+    k.energy = p.energy_per_cell_erg;
+    k.pl_slope = p.power_law_slope;
+    k.nu_min = p.nu_min_hz;
+    k.nu_max = p.nu_max_hz;
+    k.nu_custom = p.custom_frequency_hz;
+    k.seed = p.scattering_seed + static_cast<uint64_t>(p.rank);
+    k.integrator = p.integrator;
+    k.image_mode = p.mode == GRT_MODE_IMAGE;
+    // integrate_cart_ks.hpp:446-452: physics flags are gated on fluid availability.
+    k.abs_on = p.absorption_enabled && c->fluid_available;
+    k.emis_on = p.emission_enabled && c->fluid_available;
+    k.scat_on = p.scattering_enabled && c->fluid_available;
+    k.generator = p.generator;
+    // camera_plane_crossing basis (integrate_cart_ks.hpp:97-107), host libm.
+    k.cam_D = p.camera_distance;
+    k.cam_W = p.camera_width;
+    k.cam_H = p.camera_height;
+    k.cam_n[0] = std::sin(p.camera_theta) * std::cos(p.camera_phi);
+    k.cam_n[1] = std::sin(p.camera_theta) * std::sin(p.camera_phi);
+    k.cam_n[2] = std::cos(p.camera_theta);
+    k.cam_th[0] = std::cos(p.camera_theta) * std::cos(p.camera_phi);
+    k.cam_th[1] = std::cos(p.camera_theta) * std::sin(p.camera_phi);
+    k.cam_th[2] = -std::sin(p.camera_theta);
+    k.cam_ph[0] = -std::sin(p.camera_phi);
+    k.cam_ph[1] = std::cos(p.camera_phi);
+    k.cam_ph[2] = 0.0;
+    grt::KGrid& g = k.grid;
+    g.nr = c->nr;
+    g.nth = c->nth;
+    g.nph = c->nph;
+    g.available = c->fluid_available;
+    g.separable = c->separable;
+    g.r_axis = c->r_axis.ptr;
+    g.th_axis = c->th_axis.ptr;
+    g.ph_axis = c->ph_axis.ptr;
+    g.r3 = c->r3.ptr;
+    g.th3 = c->th3.ptr;
+    g.ph3 = c->ph3.ptr;
+    g.rho_t = c->rho_t.ptr;
+    g.vel = c->vel.ptr;
+    g.mag = c->mag.ptr;
+    g.r_reject_lo = c->r_reject_lo;
+    g.r_reject_hi = c->r_reject_hi;
+    k.ph = c->ph.view();
+    k.n = c->n;
+    k.counters = c->counters.ptr;
+    k.refill_threshold = c->lc.refill_threshold;
+    k.grab = c->lc.photons_per_grab;
+    k.fp64_radius_sq = 16.0 * p.mass * p.mass + p.spin * p.spin;
+    k.fp64_axis_sin2 = 0.01;
+    // FP32 right-hand side for RK45 calls outside the fluid grid (lookup can
+    // never accept radii above r_reject_hi); without a grid, everywhere.
+    k.fp32_min_radius_sq = c->fluid_available ? (std::isfinite(c->r_reject_hi) ? c->r_reject_hi * c->r_reject_hi : INFINITY) : 0.0;
+    k.renormalize = 1;
+    return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t grt_abi_version(void) { return GRT_ABI_VERSION; }
+
+const char* grt_build_info(void) {
+    return "gr-ray-tracer-b200 hot path; sm_100a; FP64 parity kernels built with -fmad=false";
+}
+
+const char* grt_last_error(const grt_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+grt_status grt_create(const grt_params* p, grt_ctx** out) {
+    if (!p || !out) return GRT_EINVAL;
+    *out = nullptr;
+    char buf[512];
+    if (grt_params_validate(p, buf, sizeof(buf)) != GRT_OK) return GRT_EINVAL;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GRT_ENODEV;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return GRT_ENODEV;
+    if (prop.major < 10) return GRT_ENODEV;
+    grt_ctx* c = new grt_ctx();
+    c->p = *p;
+    c->device = dev;
+    c->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        c->counters.alloc(1) != cudaSuccess || c->scratch_u64.alloc(4) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void**>(&c->host_counters), sizeof(grt::KCounters)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void**>(&c->host_u64), 4 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        grt_destroy(c);
+        return GRT_ECUDA;
+    }
+    c->stream = c->own_stream;
+    c->lc.blocks_per_sm = 1;
+    *out = c;
+    return GRT_OK;
+}
+
+void grt_destroy(grt_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->r_axis.release(); c->th_axis.release(); c->ph_axis.release();
+    c->r3.release(); c->th3.release(); c->ph3.release();
+    c->rho_t.release(); c->vel.release(); c->mag.release();
+    c->ph.release();
+    c->counters.release();
+    c->image.release(); c->spectrum.release(); c->arrived.release(); c->scratch_u64.release();
+    if (c->host_counters) cudaFreeHost(c->host_counters);
+    if (c->host_u64) cudaFreeHost(c->host_u64);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+grt_status grt_set_params(grt_ctx* c, const grt_params* p) {
+    if (!c || !p) return GRT_EINVAL;
+    char buf[512];
+    if (grt_params_validate(p, buf, sizeof(buf)) != GRT_OK) return fail(c, GRT_EINVAL, buf);
+    c->p = *p;
+    return GRT_OK;
+}
+
+grt_status grt_set_stream(grt_ctx* c, void* stream) {
+    if (!c) return GRT_EINVAL;
+    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+    return GRT_OK;
+}
+
+grt_status grt_synchronize(grt_ctx* c) {
+    if (!c) return GRT_EINVAL;
+    GRT_CUDA(c, cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    return GRT_OK;
+}
+
+grt_status grt_get_launch_config(const grt_ctx* c, grt_launch_config* cfg) {
+    if (!c || !cfg) return GRT_EINVAL;
+    *cfg = c->lc;
+    return GRT_OK;
+}
+
+grt_status grt_set_launch_config(grt_ctx* c, const grt_launch_config* cfg) {
+    if (!c || !cfg) return GRT_EINVAL;
+    if (cfg->threads_per_block < 32 || cfg->threads_per_block > 256 || cfg->threads_per_block % 32 != 0)
+        return fail(c, GRT_EINVAL, "threads_per_block must be a multiple of 32 in [32, 256]");
+    if (cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 32)
+        return fail(c, GRT_EINVAL, "blocks_per_sm must be in [1, 32]");
+    if (cfg->refill_threshold < 1 || cfg->refill_threshold > 32)
+        return fail(c, GRT_EINVAL, "refill_threshold must be in [1, 32]");
+    if (cfg->photons_per_grab < 1 || cfg->photons_per_grab > (1 << 20))
+        return fail(c, GRT_EINVAL, "photons_per_grab must be in [1, 2^20]");
+    c->lc = *cfg;
+    return GRT_OK;
+}
+
+grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const double* r, const double* th,
+                           const double* ph, const double* rho, const double* T, const double* vel4,
+                           const double* mag4) {
+    if (!c) return GRT_EINVAL;
+    const size_t ncell = nr * nth * nph;
+    c->grid_uploaded = true;
+    c->fluid_available = false;
+    c->separable = false;
+    c->nr = c->nth = c->nph = 0;
+    if (ncell == 0) return GRT_OK;  // vacuum: fluid_available stays false
+    if (!r || !th || !ph || !rho || !T || !vel4 || !mag4) return fail(c, GRT_EINVAL, "null grid array");
+    if (nr > (1u << 30) || nth > (1u << 30) || nph > (1u << 30) || ncell > (1ull << 31))
+        return fail(c, GRT_EINVAL, "grid too large for 32-bit cell indices");
+    c->nr = static_cast<int>(nr);
+    c->nth = static_cast<int>(nth);
+    c->nph = static_cast<int>(nph);
+    // Separable sorted coordinates -> per-axis binary-search lookup; otherwise
+    // the reference's coordinate-descent scans over the full arrays.
+    std::vector<double> ra(nr), ta(nth), pa(nph);
+    for (size_t i = 0; i < nr; ++i) ra[i] = r[i * nth * nph];
+    for (size_t j = 0; j < nth; ++j) ta[j] = th[j * nph];
+    for (size_t k = 0; k < nph; ++k) pa[k] = ph[k];
+    bool sep = true;
+    for (size_t i = 0; i < nr && sep; ++i)
+        for (size_t j = 0; j < nth && sep; ++j)
+            for (size_t k = 0; k < nph && sep; ++k) {
+                const size_t q = (i * nth + j) * nph + k;
+                if (!(r[q] == ra[i]) || !(th[q] == ta[j]) || !(ph[q] == pa[k])) sep = false;
+            }
+    sep = sep && well_separated_increasing(ra) && well_separated_increasing(ta) &&
+          well_separated_increasing(pa) && ra[0] > 0.0 && pa[0] >= 0.0 && pa[nph - 1] < 2.0 * kPi;
+    c->separable = sep;
+    // Radii outside [lo, hi] fail within_radial_cell for every cell (margin
+    // 0.6 > 0.500001 of the outermost log spacing), so lookup can stop early.
+    c->r_reject_lo = 0.0;
+    c->r_reject_hi = INFINITY;
+    if (sep && nr >= 2) {
+        const double span_lo = std::fabs(std::log(ra[0] / ra[1]));
+        const double span_hi = std::fabs(std::log(ra[nr - 1] / ra[nr - 2]));
+        c->r_reject_lo = ra[0] * std::exp(-0.6 * span_lo);
+        c->r_reject_hi = ra[nr - 1] * std::exp(0.6 * span_hi);
+    }
+    std::vector<double2> rt(ncell), uv(2 * ncell), bv(2 * ncell);
+    for (size_t q = 0; q < ncell; ++q) {
+        rt[q] = make_double2(rho[q], T[q]);
+        double u[4], b[4];
+        spherical_to_cartesian_vec(r[q], th[q], ph[q], c->p.spin, vel4 + 4 * q, c->p.four_velocity_cm_s_per_code, u);
+        spherical_to_cartesian_vec(r[q], th[q], ph[q], c->p.spin, mag4 + 4 * q, c->p.magnetic_gauss_per_code, b);
+        uv[2 * q] = make_double2(u[0], u[1]);
+        uv[2 * q + 1] = make_double2(u[2], u[3]);
+        bv[2 * q] = make_double2(b[0], b[1]);
+        bv[2 * q + 1] = make_double2(b[2], b[3]);
+    }
+    GRT_CUDA(c, c->rho_t.alloc(ncell), "alloc rho_t");
+    GRT_CUDA(c, c->vel.alloc(2 * ncell), "alloc vel");
+    GRT_CUDA(c, c->mag.alloc(2 * ncell), "alloc mag");
+    GRT_CUDA(c, c->r_axis.alloc(nr), "alloc axis");
+    GRT_CUDA(c, c->th_axis.alloc(nth), "alloc axis");
+    GRT_CUDA(c, c->ph_axis.alloc(nph), "alloc axis");
+    GRT_CUDA(c, cudaMemcpy(c->rho_t.ptr, rt.data(), ncell * sizeof(double2), cudaMemcpyHostToDevice), "H2D grid");
+    GRT_CUDA(c, cudaMemcpy(c->vel.ptr, uv.data(), 2 * ncell * sizeof(double2), cudaMemcpyHostToDevice), "H2D grid");
+    GRT_CUDA(c, cudaMemcpy(c->mag.ptr, bv.data(), 2 * ncell * sizeof(double2), cudaMemcpyHostToDevice), "H2D grid");
+    GRT_CUDA(c, cudaMemcpy(c->r_axis.ptr, ra.data(), nr * sizeof(double), cudaMemcpyHostToDevice), "H2D axis");
+    GRT_CUDA(c, cudaMemcpy(c->th_axis.ptr, ta.data(), nth * sizeof(double), cudaMemcpyHostToDevice), "H2D axis");
+    GRT_CUDA(c, cudaMemcpy(c->ph_axis.ptr, pa.data(), nph * sizeof(double), cudaMemcpyHostToDevice), "H2D axis");
+    if (!sep) {
+        GRT_CUDA(c, c->r3.alloc(ncell), "alloc r3");
+        GRT_CUDA(c, c->th3.alloc(ncell), "alloc th3");
+        GRT_CUDA(c, c->ph3.alloc(ncell), "alloc ph3");
+        GRT_CUDA(c, cudaMemcpy(c->r3.ptr, r, ncell * sizeof(double), cudaMemcpyHostToDevice), "H2D r3");
+        GRT_CUDA(c, cudaMemcpy(c->th3.ptr, th, ncell * sizeof(double), cudaMemcpyHostToDevice), "H2D th3");
+        GRT_CUDA(c, cudaMemcpy(c->ph3.ptr, ph, ncell * sizeof(double), cudaMemcpyHostToDevice), "H2D ph3");
+    }
+    c->fluid_available = true;
+    return GRT_OK;
+}
+
+grt_status grt_upload_grid_numpy_dir(grt_ctx* c, const char* dir) {
+    if (!c || !dir) return GRT_EINVAL;
+    namespace fs = std::filesystem;
+    const fs::path root(dir);
+    if (!fs::exists(root)) return fail(c, GRT_EIO, "NumPy directory does not exist: " + root.string());
+    if (!fs::is_directory(root)) return fail(c, GRT_EIO, "NumPy input path is not a directory: " + root.string());
+    const char* names[7] = {"r.npy", "theta.npy", "phi.npy", "rho.npy", "Tgas.npy", "vel.npy", "mag.npy"};
+    std::string missing;
+    for (const char* n : names)
+        if (!fs::is_regular_file(root / n)) missing += (missing.empty() ? "" : ", ") + std::string(n);
+    if (!missing.empty())
+        return fail(c, GRT_EIO, "NumPy directory '" + root.string() + "' is missing required file(s): " + missing);
+    std::vector<double> a[7];
+    std::vector<size_t> shape[7];
+    for (int q = 0; q < 7; ++q) {
+        std::string e;
+        if (!grt::npy_load_f64((root / names[q]).string(), shape[q], a[q], e)) return fail(c, GRT_EIO, e);
+    }
+    const std::vector<size_t>& s0 = shape[0];
+    if (s0.size() != 3 || s0[0] == 0 || s0[1] == 0 || s0[2] == 0)
+        return fail(c, GRT_EINVAL, "Coordinate grid must have shape (nr, ntheta, nphi): " + (root / names[0]).string());
+    for (int q = 1; q < 7; ++q) {
+        const size_t dims = q >= 5 ? 4 : 3;
+        if (shape[q].size() != dims || shape[q][0] != s0[0] || shape[q][1] != s0[1] || shape[q][2] != s0[2])
+            return fail(c, GRT_EINVAL, std::string("Grid field has incompatible dimensions: ") + (root / names[q]).string());
+        if (dims == 4 && shape[q][3] != 4)
+            return fail(c, GRT_EINVAL, std::string("Four-vector field must have four components: ") + (root / names[q]).string());
+    }
+    return grt_upload_grid(c, s0[0], s0[1], s0[2], a[0].data(), a[1].data(), a[2].data(), a[3].data(), a[4].data(),
+                           a[5].data(), a[6].data());
+}
+
+static grt_status count_initial_terminated(grt_ctx* c) {
+    GRT_CUDA(c, cudaMemsetAsync(c->scratch_u64.ptr, 0, sizeof(unsigned long long), c->stream), "memset");
+    GRT_CUDA(c, grt::launch_count_terminated(c->ph.term.ptr, c->n, c->scratch_u64.ptr, c->sm_count, c->stream),
+             "count_terminated");
+    GRT_CUDA(c, cudaMemcpyAsync(c->host_u64, c->scratch_u64.ptr, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                c->stream), "D2H count");
+    GRT_CUDA(c, cudaStreamSynchronize(c->stream), "sync");
+    c->initial_terminated = c->host_u64[0];
+    return GRT_OK;
+}
+
+grt_status grt_upload_photons(grt_ctx* c, const grt_photon_soa* s, size_t n) {
+    if (!c || (!s && n)) return GRT_EINVAL;
+    if (n > (1ull << 40)) return fail(c, GRT_EINVAL, "photon count too large");
+    GRT_CUDA(c, c->ph.alloc(n), "alloc photons");
+    c->n = n;
+    if (n == 0) {
+        c->initial_terminated = 0;
+        return GRT_OK;
+    }
+    double* src[17];
+    soa_doubles(s, src);
+    if (!s->id || !s->terminate || !s->phase) return fail(c, GRT_EINVAL, "null photon field");
+    for (double* q : src)
+        if (!q) return fail(c, GRT_EINVAL, "null photon field");
+    GRT_CUDA(c, cudaMemcpyAsync(c->ph.id.ptr, s->id, n * 8, cudaMemcpyHostToDevice, c->stream), "H2D id");
+    for (int q = 0; q < 17; ++q)
+        GRT_CUDA(c, cudaMemcpyAsync(c->ph.f[q].ptr, src[q], n * 8, cudaMemcpyHostToDevice, c->stream), "H2D photons");
+    GRT_CUDA(c, cudaMemcpyAsync(c->ph.term.ptr, s->terminate, n, cudaMemcpyHostToDevice, c->stream), "H2D term");
+    GRT_CUDA(c, cudaMemcpyAsync(c->ph.phase.ptr, s->phase, n, cudaMemcpyHostToDevice, c->stream), "H2D phase");
+    return count_initial_terminated(c);
+}
+
+size_t grt_photon_count(const grt_ctx* c) { return c ? c->n : 0; }
+
+grt_status grt_download_photons(grt_ctx* c, grt_photon_soa* s) {
+    if (!c || !s) return GRT_EINVAL;
+    const size_t n = c->n;
+    if (n == 0) return GRT_OK;
+    double* dst[17];
+    soa_doubles(s, dst);
+    if (s->id) GRT_CUDA(c, cudaMemcpyAsync(s->id, c->ph.id.ptr, n * 8, cudaMemcpyDeviceToHost, c->stream), "D2H");
+    for (int q = 0; q < 17; ++q)
+        if (dst[q]) GRT_CUDA(c, cudaMemcpyAsync(dst[q], c->ph.f[q].ptr, n * 8, cudaMemcpyDeviceToHost, c->stream), "D2H");
+    if (s->terminate) GRT_CUDA(c, cudaMemcpyAsync(s->terminate, c->ph.term.ptr, n, cudaMemcpyDeviceToHost, c->stream), "D2H");
+    if (s->phase) GRT_CUDA(c, cudaMemcpyAsync(s->phase, c->ph.phase.ptr, n, cudaMemcpyDeviceToHost, c->stream), "D2H");
+    GRT_CUDA(c, cudaStreamSynchronize(c->stream), "sync");
+    return GRT_OK;
+}
+
+grt_status grt_init_image_photons(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t id_offset) {
+    if (!c) return GRT_EINVAL;
+    const size_t n = static_cast<size_t>(nx * ny);
+    GRT_CUDA(c, c->ph.alloc(n), "alloc photons");
+    c->n = n;
+    c->initial_terminated = 0;
+    const grt_params& p = c->p;
+    grt::InitImageArgs a;
+    a.ph = c->ph.view();
+    a.offset = 0;
+    a.nx = nx;
+    a.ny = ny;
+    a.id_offset = id_offset;
+    a.W = p.camera_width;
+    a.H = p.camera_height;
+    // initialize_photons.hpp:94-108, evaluated on the host exactly as there.
+    a.cx = p.camera_distance * std::sin(p.camera_theta) * std::cos(p.camera_phi);
+    a.cy = p.camera_distance * std::sin(p.camera_theta) * std::sin(p.camera_phi);
+    a.cz = p.camera_distance * std::cos(p.camera_theta);
+    a.th_hat[0] = std::cos(p.camera_theta) * std::cos(p.camera_phi);
+    a.th_hat[1] = std::cos(p.camera_theta) * std::sin(p.camera_phi);
+    a.th_hat[2] = -std::sin(p.camera_theta);
+    a.ph_hat[0] = -std::sin(p.camera_phi);
+    a.ph_hat[1] = std::cos(p.camera_phi);
+    a.ph_hat[2] = 0.0;
+    a.a = p.spin;
+    a.M = p.mass;
+    a.dlambda0 = p.initial_step * p.camera_distance;
+    GRT_CUDA(c, grt::launch_init_image(a, c->stream), "init_image_pixels");
+    return GRT_OK;
+}
+
+grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
+    if (!c) return GRT_EINVAL;
+    if (!c->grid_uploaded) return fail(c, GRT_ESTATE, "grt_run before grt_upload_grid");
+    const grt_params& p = c->p;
+    grt_run_stats st;
+    std::memset(&st, 0, sizeof(st));
+    if (c->n == 0) {
+        st.steps_done = p.max_steps;
+        if (stats) *stats = st;
+        return GRT_OK;
+    }
+    grt::KParams kp = make_kparams(c);
+    const size_t smem = c->separable ? (c->nr + c->nth + c->nph) * sizeof(double) : 0;
+    const int threads = c->lc.threads_per_block;
+    const int blocks = c->sm_count * c->lc.blocks_per_sm;
+    const unsigned long long total = c->n;
+    unsigned long long terminated = c->initial_terminated;
+    const uint64_t interval = p.output_interval ? p.output_interval : 1;
+    // Chunks end on the reference's output steps (step % interval == 0 or the
+    // last step), where it evaluates the termination fraction
+    // (integrate_cart_ks.hpp:491-526).  With termination_percent = 1 the check
+    // can only succeed once every photon has terminated, so one launch covers
+    // the whole loop.
+    const bool single = p.termination_percent >= 1.0;
+    int64_t step = 0;
+    int64_t steps_done = 0;
+    unsigned long long max_term_step = 0;
+    float ms_total = 0.0f;
+    while (step < p.max_steps) {
+        int64_t end;
+        if (single) {
+            end = p.max_steps;
+        } else {
+            // next output step at or after `step`
+            int64_t next = static_cast<int64_t>(((static_cast<uint64_t>(step) + interval - 1) / interval) * interval);
+            if (next > p.max_steps - 1) next = p.max_steps - 1;
+            end = next + 1;
+        }
+        kp.step0 = step;
+        kp.budget = end - step;
+        const unsigned long long warps = static_cast<unsigned long long>(blocks) * (threads / 32);
+        kp.max_iterations = static_cast<unsigned long long>(kp.budget + 2) * 13ull *
+                                ((total + warps - 1) / warps + static_cast<unsigned long long>(kp.grab)) +
+                            (1ull << 20);
+        GRT_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, sizeof(grt::KCounters), c->stream), "memset counters");
+        GRT_CUDA(c, cudaEventRecord(c->ev0, c->stream), "event");
+        cudaError_t e = p.precision == GRT_PREC_MIXED
+                            ? grt::launch_trace_mixed(kp, p.integrator, blocks, threads, smem, c->stream)
+                            : grt::launch_trace_fp64(kp, p.integrator, blocks, threads, smem, c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "trace launch");
+        GRT_CUDA(c, cudaEventRecord(c->ev1, c->stream), "event");
+        GRT_CUDA(c, cudaMemcpyAsync(c->host_counters, c->counters.ptr, sizeof(grt::KCounters), cudaMemcpyDeviceToHost,
+                                    c->stream), "D2H counters");
+        GRT_CUDA(c, cudaStreamSynchronize(c->stream), "trace kernel");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        ms_total += ms;
+        const grt::KCounters& k = *c->host_counters;
+        terminated += k.terminated;
+        st.accepted_steps += k.accepted;
+        st.rejected_attempts += k.rejected;
+        st.photon_calls += k.calls;
+        st.launches += 1;
+        if (k.max_term_step > max_term_step) max_term_step = k.max_term_step;
+        if (k.timed_out) {
+            st.timed_out = 1;
+            st.trace_ms = ms_total;
+            st.n_terminated = terminated;
+            if (stats) *stats = st;
+            return fail(c, GRT_ETIMEOUT, "trace kernel hit its iteration limit");
+        }
+        step = end;
+        steps_done = end;
+        const double fraction = static_cast<double>(terminated) / static_cast<double>(total);
+        if (fraction >= p.termination_percent) break;
+    }
+    if (single && terminated >= total) {
+        // The reference stops after the first output step at or after the last termination.
+        const int64_t last = max_term_step ? static_cast<int64_t>(max_term_step) - 1 : 0;
+        int64_t s_out = static_cast<int64_t>(((static_cast<uint64_t>(last) + interval - 1) / interval) * interval);
+        if (s_out > p.max_steps - 1) s_out = p.max_steps - 1;
+        steps_done = s_out + 1;
+    }
+    st.steps_done = steps_done;
+    st.n_terminated = terminated;
+    st.trace_ms = ms_total;
+    if (stats) *stats = st;
+    return GRT_OK;
+}
+
+grt_status grt_get_image_products(grt_ctx* c, grt_image_products* out) {
+    if (!c || !out) return GRT_EINVAL;
+    const grt_params& p = c->p;
+    const size_t npix = p.image_nx * p.image_ny, bins = p.spectrum_bins;
+    if (!out->image_I || !out->image_Q || !out->image_U || !out->image_V || !out->spectrum_frequency_hz ||
+        !out->spectrum_I || !out->arrived_count)
+        return fail(c, GRT_EINVAL, "null image product buffer");
+    GRT_CUDA(c, c->image.alloc(4 * npix), "alloc image");
+    GRT_CUDA(c, c->spectrum.alloc(bins), "alloc spectrum");
+    GRT_CUDA(c, c->arrived.alloc(1), "alloc arrived");
+    GRT_CUDA(c, cudaMemsetAsync(c->image.ptr, 0, 4 * npix * sizeof(double), c->stream), "memset");
+    GRT_CUDA(c, cudaMemsetAsync(c->spectrum.ptr, 0, bins * sizeof(double), c->stream), "memset");
+    GRT_CUDA(c, cudaMemsetAsync(c->arrived.ptr, 0, sizeof(unsigned long long), c->stream), "memset");
+    const double log_min = std::log10(p.spectrum_min_hz), log_max = std::log10(p.spectrum_max_hz);
+    grt::ProductsArgs a;
+    a.ph = c->ph.view();
+    a.offset = 0;
+    a.n = c->n;
+    a.nx = p.image_nx;
+    a.ny = p.image_ny;
+    a.bins = bins;
+    a.W = p.camera_width;
+    a.H = p.camera_height;
+    a.spec_min = p.spectrum_min_hz;
+    a.spec_max = p.spectrum_max_hz;
+    a.log_min = log_min;
+    a.log_max = log_max;
+    a.image = c->image.ptr;
+    a.spectrum = c->spectrum.ptr;
+    a.arrived = c->arrived.ptr;
+    GRT_CUDA(c, grt::launch_image_products(a, c->stream), "image_products");
+    double* dst[4] = {out->image_I, out->image_Q, out->image_U, out->image_V};
+    for (int q = 0; q < 4; ++q)
+        GRT_CUDA(c, cudaMemcpyAsync(dst[q], c->image.ptr + q * npix, npix * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream), "D2H image");
+    GRT_CUDA(c, cudaMemcpyAsync(out->spectrum_I, c->spectrum.ptr, bins * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream), "D2H spectrum");
+    GRT_CUDA(c, cudaMemcpyAsync(out->arrived_count, c->arrived.ptr, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                c->stream), "D2H arrived");
+    // observation.hpp:51-58, on the host like the reference.
+    for (size_t b = 0; b < bins; ++b) {
+        const double f = bins > 1 ? static_cast<double>(b) / static_cast<double>(bins - 1) : 0.0;
+        out->spectrum_frequency_hz[b] = std::pow(10.0, log_min + f * (log_max - log_min));
+    }
+    GRT_CUDA(c, cudaStreamSynchronize(c->stream), "products");
+    return GRT_OK;
+}
+
+grt_status grt_write_image_products_npz(grt_ctx* c, const char* output_dir, const char* name) {
+    if (!c || !output_dir || !name) return GRT_EINVAL;
+    const grt_params& p = c->p;
+    const size_t nx = p.image_nx, ny = p.image_ny, bins = p.spectrum_bins;
+    std::vector<double> I(nx * ny), Q(nx * ny), U(nx * ny), V(nx * ny), sf(bins), si(bins);
+    uint64_t arrived = 0;
+    grt_image_products out{I.data(), Q.data(), U.data(), V.data(), sf.data(), si.data(), &arrived};
+    grt_status s = grt_get_image_products(c, &out);
+    if (s != GRT_OK) return s;
+    namespace fs = std::filesystem;
+    std::error_code ec;
+    fs::create_directories(output_dir, ec);
+    const fs::path final_path = fs::path(output_dir) / (std::string(name) + "_image_products.npz");
+    const fs::path tmp = final_path.string() + ".tmp";
+    grt::NpzOut z;
+    if (!z.open(tmp.string())) return fail(c, GRT_EIO, "Failed to open output NumPy archive: " + tmp.string());
+    const std::vector<size_t> img{ny, nx}, spec{bins}, one{1};
+    bool ok = z.add("image_I", grt::npy_bytes("<f8", img, I.data(), 8)) &&
+              z.add("image_Q", grt::npy_bytes("<f8", img, Q.data(), 8)) &&
+              z.add("image_U", grt::npy_bytes("<f8", img, U.data(), 8)) &&
+              z.add("image_V", grt::npy_bytes("<f8", img, V.data(), 8)) &&
+              z.add("spectrum_frequency_hz", grt::npy_bytes("<f8", spec, sf.data(), 8)) &&
+              z.add("spectrum_I", grt::npy_bytes("<f8", spec, si.data(), 8)) &&
+              z.add("arrived_count", grt::npy_bytes("<u8", one, &arrived, 8));
+    ok = z.close() && ok;
+    if (!ok) {
+        fs::remove(tmp, ec);
+        return fail(c, GRT_EIO, "Failed while writing NumPy archive");
+    }
+    fs::rename(tmp, final_path, ec);
+    if (ec) {
+        fs::remove(tmp, ec);
+        return fail(c, GRT_EIO, "Failed to publish output archive " + final_path.string());
+    }
+    return GRT_OK;
+}
+
+}  // extern "C"

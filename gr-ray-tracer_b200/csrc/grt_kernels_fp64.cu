@@ -1,0 +1,143 @@
+// FP64 parity-form kernels.  Built with -fmad=false so that every product and
+// sum rounds separately, as in the reference's host build.
+//
+//   trace_fp64<RK4|RK45>  -- persistent per-photon step loop (integrate_cart_ks.hpp:230-419)
+//   init_image_pixels     -- pixel-grid camera rays (initialize_photons.hpp:82-170)
+//   image_products        -- build_observation_products (observation.hpp:31-84)
+//   count_terminated      -- "Count Terminated Photons" (integrate_cart_ks.hpp:496-503)
+#include "grt_launch.h"
+#include "grt_trace.cuh"
+
+namespace grt {
+
+template <int INTEGRATOR>
+__global__ void __launch_bounds__(256) trace_fp64(const __grid_constant__ KParams kp) {
+    extern __shared__ double smem[];
+    const double *s_r, *s_th, *s_ph;
+    dev::stage_axes(kp, smem, s_r, s_th, s_ph);
+    dev::trace_body<INTEGRATOR, dev::Fp64Rhs>(kp, s_r, s_th, s_ph);
+}
+
+// initialize_photons.hpp:116-169 with screen (u, v) at pixel centres; the
+// camera centre and basis come from the host (glibc sin/cos, like the reference).
+__global__ void init_image_pixels(const __grid_constant__ InitImageArgs args) {
+    const unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
+    if (i >= args.nx * args.ny) return;
+    const unsigned long long iy = i / args.nx, ix = i % args.nx;
+    const double u = -0.5 * args.W + (static_cast<double>(ix) + 0.5) * args.W / static_cast<double>(args.nx);
+    const double v = -0.5 * args.H + (static_cast<double>(iy) + 0.5) * args.H / static_cast<double>(args.ny);
+    const double x = args.cx + u * args.th_hat[0] + v * args.ph_hat[0];
+    const double y = args.cy + u * args.th_hat[1] + v * args.ph_hat[1];
+    const double z = args.cz + u * args.th_hat[2] + v * args.ph_hat[2];
+    double kx = -args.cx, ky = -args.cy, kz = -args.cz;
+    const double kn = sqrt(kx * kx + ky * ky + kz * kz);
+    kx /= kn;
+    ky /= kn;
+    kz /= kn;
+    const double X[4] = {0.0, x, y, z};
+    const double K[3] = {kx, ky, kz};
+    double p[4] = {0.0, 0.0, 0.0, 0.0};
+    dev::ks_null_momentum(X, K, args.a, args.M, p);
+    const KPhotons& P = args.ph;
+    const unsigned long long o = args.offset + i;
+    P.id[o] = args.id_offset + i;
+    P.frequency[o] = 0.0;
+    P.emission_frame_energy[o] = 1.0;
+    P.x0[o] = 0.0; P.x1[o] = x; P.x2[o] = y; P.x3[o] = z;
+    P.k0[o] = p[0]; P.k1[o] = p[1]; P.k2[o] = p[2]; P.k3[o] = p[3];
+    P.I[o] = 0.0; P.Q[o] = 0.0; P.U[o] = 0.0; P.V[o] = 0.0;
+    P.dlambda[o] = args.dlambda0;
+    P.terminate[o] = 0;
+    P.phase[o] = 1;  // ImageBackward
+    P.theta_disp[o] = u;
+    P.phi_disp[o] = v;
+}
+
+// observation.hpp:22-29
+__device__ __forceinline__ unsigned long long observation_bin(double value, double lo, double hi,
+                                                              unsigned long long bins) {
+    if (bins <= 1 || !(hi > lo)) return 0;
+    const double f = (value - lo) / (hi - lo);
+    const double sc = fmax(0.0, fmin(1.0, f));
+    return static_cast<unsigned long long>(sc * static_cast<double>(bins - 1));
+}
+
+// observation.hpp:61-82: ImageArrived photons binned by arrival (u, v) and log10(nu).
+__global__ void image_products(const __grid_constant__ ProductsArgs args) {
+    const unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
+    bool arrived = false;
+    if (i < args.n) {
+        const unsigned long long o = args.offset + i;
+        if (args.ph.phase[o] == 3) {
+            arrived = true;
+            const unsigned long long px = observation_bin(args.ph.theta_disp[o], -0.5 * args.W, 0.5 * args.W, args.nx);
+            const unsigned long long py = observation_bin(args.ph.phi_disp[o], -0.5 * args.H, 0.5 * args.H, args.ny);
+            const unsigned long long pix = py * args.nx + px;
+            const double I = args.ph.I[o];
+            atomicAdd(&args.image[pix], I);
+            atomicAdd(&args.image[args.nx * args.ny + pix], args.ph.Q[o]);
+            atomicAdd(&args.image[2 * args.nx * args.ny + pix], args.ph.U[o]);
+            atomicAdd(&args.image[3 * args.nx * args.ny + pix], args.ph.V[o]);
+            const double f = args.ph.frequency[o];
+            if (f >= args.spec_min && f <= args.spec_max) {
+                const unsigned long long b = observation_bin(log10(f), args.log_min, args.log_max, args.bins);
+                atomicAdd(&args.spectrum[b], I);
+            }
+        }
+    }
+    const unsigned mask = __ballot_sync(0xFFFFFFFFu, arrived);
+    if ((threadIdx.x & 31) == 0 && mask) atomicAdd(args.arrived, static_cast<unsigned long long>(__popc(mask)));
+}
+
+__global__ void count_terminated(const uint8_t* __restrict__ term, unsigned long long n,
+                                 unsigned long long* out) {
+    unsigned long long c = 0;
+    for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<unsigned long long>(gridDim.x) * blockDim.x)
+        c += term[i] ? 1 : 0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, off);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+// ---- host-side launchers ----
+cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int blocks, int threads, size_t smem,
+                              cudaStream_t stream) {
+    if (integrator == 0) {
+        cudaFuncSetAttribute(trace_fp64<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        trace_fp64<0><<<blocks, threads, smem, stream>>>(kp);
+    } else {
+        cudaFuncSetAttribute(trace_fp64<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        trace_fp64<1><<<blocks, threads, smem, stream>>>(kp);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_image(const InitImageArgs& args, cudaStream_t stream) {
+    const unsigned long long n = args.nx * args.ny;
+    if (n == 0) return cudaSuccess;
+    const unsigned threads = 256;
+    const unsigned blocks = static_cast<unsigned>((n + threads - 1) / threads);
+    init_image_pixels<<<blocks, threads, 0, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_image_products(const ProductsArgs& args, cudaStream_t stream) {
+    if (args.n == 0) return cudaSuccess;
+    const unsigned threads = 256;
+    const unsigned blocks = static_cast<unsigned>((args.n + threads - 1) / threads);
+    image_products<<<blocks, threads, 0, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_terminated(const uint8_t* term, unsigned long long n, unsigned long long* out,
+                                    int sm_count, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    unsigned long long want = (n + 255) / 256;
+    const unsigned long long cap = static_cast<unsigned long long>(sm_count) * 8;
+    const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
+    count_terminated<<<blocks, 256, 0, stream>>>(term, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace grt

@@ -1,0 +1,92 @@
+// Parameter block passed by value to the trace kernels (one __grid_constant__
+// struct per launch), built on the host from grt_params by grt_api.cu.
+#pragma once
+
+#include <stdint.h>
+#include <vector_types.h>
+
+namespace grt {
+
+// Device view of the fluid grid (replaces ScatteringFluidGrid,
+// src/radiative_transfer/scattering.hpp:22-39).
+struct KGrid {
+    int nr, nth, nph;
+    int available;   // fluid present (integrate_cart_ks.hpp:436-445)
+    int separable;   // coordinates are sorted per-axis products (fast lookup path)
+    int pad;
+    const double* r_axis;   // [nr]   separable axes (staged into shared memory)
+    const double* th_axis;  // [nth]
+    const double* ph_axis;  // [nph]
+    const double* r3;       // [nr*nth*nph] full coordinates (general path)
+    const double* th3;
+    const double* ph3;
+    const double2* rho_t;   // [ncells] (rho, T) in code units
+    const double2* vel;     // [2*ncells] Cartesian KS u^mu * velocity scale
+    const double2* mag;     // [2*ncells] Cartesian KS b^mu * magnetic scale
+    double r_reject_lo;     // radii outside [lo, hi] cannot pass within_radial_cell
+    double r_reject_hi;
+};
+
+// Device structure-of-arrays photon state (struct Photons, src/utils.hpp:40-133).
+struct KPhotons {
+    uint64_t* id;
+    double* frequency;
+    double* emission_frame_energy;
+    double* x0; double* x1; double* x2; double* x3;
+    double* k0; double* k1; double* k2; double* k3;
+    double* I; double* Q; double* U; double* V;
+    double* dlambda;
+    double* theta_disp;
+    double* phi_disp;
+    uint8_t* terminate;
+    uint8_t* phase;
+};
+
+// Counters one trace launch accumulates (all zeroed before the launch).
+struct KCounters {
+    unsigned long long queue_head;        // next photon index to hand out
+    unsigned long long terminated;        // photons that terminated in this launch
+    unsigned long long accepted;          // accepted ray-steps
+    unsigned long long rejected;          // rejected RK45 attempts
+    unsigned long long calls;             // functor invocations on live photons
+    unsigned long long max_term_step;     // largest global step index at which a photon terminated, +1
+    unsigned long long timed_out;         // warps that hit their iteration limit
+    unsigned long long pad;
+};
+
+struct KParams {
+    // physics
+    double a, M;
+    double r_min, r_max;
+    double atol, rtol, min_scale, max_scale, safety;
+    double kappa, jcoef, albedo;
+    double length_scale, time_scale, density_scale, temperature_scale;
+    double norm, energy, pl_slope, nu_min, nu_max, nu_custom;
+    uint64_t seed;             // scattering.seed + rank
+    int integrator;            // GRT_RK4 / GRT_RK45
+    int image_mode;            // simulation.mode == image
+    int abs_on, emis_on, scat_on;  // already ANDed with fluid availability
+    int generator;
+    // camera plane basis (integrate_cart_ks.hpp:96-107), computed on the host
+    double cam_D, cam_W, cam_H;
+    double cam_n[3], cam_th[3], cam_ph[3];
+    KGrid grid;
+    KPhotons ph;
+    uint64_t n;                // photons in the queue
+    int64_t step0;             // global step index of this launch's first call
+    int64_t budget;            // calls each live photon may take in this launch
+    unsigned long long max_iterations;  // per-warp loop limit (GRT_ETIMEOUT)
+    KCounters* counters;
+    int refill_threshold;      // idle lanes before a warp refills (1..32)
+    int grab;                  // photons claimed per queue access (per warp)
+    const double* m_abs;       // optional per-cell multipliers on dtau (nullptr = 1)
+    const double* m_emis;      // optional per-cell multipliers on dI
+    // mixed-precision form only
+    double fp64_radius_sq;     // x^2+y^2+z^2 below this uses the FP64 right-hand side
+    double fp64_axis_sin2;     // (x^2+y^2)/(x^2+y^2+z^2) below this (polar axis) uses FP64
+    double fp32_min_radius_sq; // RK45 calls start r^2 above this (outside the fluid grid) for FP32
+    int renormalize;           // restore g^{mu nu} p_mu p_nu = 0 in FP64 after each accepted step
+    int pad2;
+};
+
+}  // namespace grt

@@ -1,0 +1,44 @@
+// Host-side launch interface between the C ABI (grt_api.cu) and the kernel
+// translation units.  Internal to the library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "grt_kparams.h"
+
+namespace grt {
+
+struct InitImageArgs {
+    KPhotons ph;
+    unsigned long long offset;     // first photon slot written
+    unsigned long long nx, ny;
+    unsigned long long id_offset;
+    double W, H;
+    double cx, cy, cz;
+    double th_hat[3], ph_hat[3];
+    double a, M;
+    double dlambda0;               // initial_step * camera_distance
+};
+
+struct ProductsArgs {
+    KPhotons ph;
+    unsigned long long offset, n;  // photon slots [offset, offset + n)
+    unsigned long long nx, ny, bins;
+    double W, H;
+    double spec_min, spec_max, log_min, log_max;
+    double* image;                 // [4][ny][nx] (I, Q, U, V)
+    double* spectrum;              // [bins]
+    unsigned long long* arrived;   // [1]
+};
+
+cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int blocks, int threads, size_t smem,
+                              cudaStream_t stream);
+cudaError_t launch_trace_mixed(const KParams& kp, int integrator, int blocks, int threads, size_t smem,
+                               cudaStream_t stream);
+cudaError_t launch_init_image(const InitImageArgs& args, cudaStream_t stream);
+cudaError_t launch_image_products(const ProductsArgs& args, cudaStream_t stream);
+cudaError_t launch_count_terminated(const uint8_t* term, unsigned long long n, unsigned long long* out,
+                                    int sm_count, cudaStream_t stream);
+
+}  // namespace grt

@@ -1,0 +1,462 @@
+// Persistent trace kernel body, templated on the right-hand-side policy.
+//
+// Replaces the host step loop's per-step launch of the reference functor
+// (src/geodesic_integrate/integrate_cart_ks.hpp:468-481, operator() :230-419):
+// one launch advances every photon by up to `budget` functor invocations
+// ("calls"), keeping its state in registers between calls.  Photons are
+// independent, so this is exactly the reference's result whenever no
+// termination check falls inside the launch (the host splits launches at the
+// reference's output steps when termination_percent < 1).
+//
+// Work distribution: each warp claims contiguous blocks of `grab` photon
+// indices from a global queue; lanes whose photon terminated (or used its
+// budget) stay idle until at least `refill_threshold` lanes are idle, then the
+// warp hands them the next indices with one ballot + prefix rank.  A loop
+// iteration is one unit of work per lane: a complete RK4 call, or one RK45
+// attempt (rejected attempts no longer hold the whole warp for 12 tries).
+#pragma once
+
+#include "grt_device.cuh"
+#include "grt_fourth_root.cuh"
+
+namespace grt {
+namespace dev {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// Fehlberg 4(5) tableau (integrate_cart_ks.hpp:166-180).
+constexpr double a21 = 1.0 / 4.0;
+constexpr double a31 = 3.0 / 32.0, a32 = 9.0 / 32.0;
+constexpr double a41 = 1932.0 / 2197.0, a42 = -7200.0 / 2197.0, a43 = 7296.0 / 2197.0;
+constexpr double a51 = 439.0 / 216.0, a52 = -8.0, a53 = 3680.0 / 513.0, a54 = -845.0 / 4104.0;
+constexpr double a61 = -8.0 / 27.0, a62 = 2.0, a63 = -3544.0 / 2565.0, a64 = 1859.0 / 4104.0,
+                 a65 = -11.0 / 40.0;
+constexpr double b41 = 25.0 / 216.0, b43 = 1408.0 / 2565.0, b44 = 2197.0 / 4104.0, b45 = -1.0 / 5.0;
+constexpr double b51 = 16.0 / 135.0, b53 = 6656.0 / 12825.0, b54 = 28561.0 / 56430.0,
+                 b55 = -9.0 / 50.0, b56 = 2.0 / 55.0;
+
+// The seven evolving components of the state (t,x,y,z,px,py,pz); p_t is constant.
+struct V7 {
+    double v[7];
+};
+
+GRT_DEV V7 to_v7(const Rhs7& r) {
+    V7 o;
+    o.v[0] = r.t; o.v[1] = r.x; o.v[2] = r.y; o.v[3] = r.z;
+    o.v[4] = r.px; o.v[5] = r.py; o.v[6] = r.pz;
+    return o;
+}
+
+// state index of V7 component c
+GRT_DEV constexpr int sidx(int c) { return c < 4 ? c : c + 1; }
+
+// Right-hand-side policy of the FP64 parity form.
+// `fast` is the per-call precision hint of the mixed form (ignored here).
+struct Fp64Rhs {
+    static GRT_DEV V7 eval(const double s[8], const KParams& kp, int /*fast*/) {
+        return to_v7(ks_rhs(s[1], s[2], s[3], s[4], s[5], s[6], s[7], kp.a, kp.M));
+    }
+    static GRT_DEV void after_accept(double*, const KParams&, int) {}
+};
+
+struct Lane {
+    double s[8];
+    double I[4];
+    double freq, emit, dl;
+    double radius;        // ks_radius of s, valid when have_radius
+    uint64_t id;
+    long long idx;        // photon index, -1 when idle
+    long long calls;      // calls taken in this launch
+    int phase;
+    int have_radius;
+    // RK45 call in progress
+    int mid_call;
+    int attempts;
+    int fast;             // precision hint of the current call (mixed form)
+    double dl_try;
+    V7 k1;
+};
+
+GRT_DEV void load_photon(const KPhotons& P, long long i, Lane& L) {
+    L.id = P.id[i];
+    L.freq = P.frequency[i];
+    L.emit = P.emission_frame_energy[i];
+    L.s[0] = P.x0[i]; L.s[1] = P.x1[i]; L.s[2] = P.x2[i]; L.s[3] = P.x3[i];
+    L.s[4] = P.k0[i]; L.s[5] = P.k1[i]; L.s[6] = P.k2[i]; L.s[7] = P.k3[i];
+    L.I[0] = P.I[i]; L.I[1] = P.Q[i]; L.I[2] = P.U[i]; L.I[3] = P.V[i];
+    L.dl = P.dlambda[i];
+    L.phase = P.phase[i];
+    L.calls = 0;
+    L.have_radius = 0;
+    L.mid_call = 0;
+}
+
+GRT_DEV void store_photon(const KPhotons& P, const Lane& L, int terminated, double tdisp, double pdisp,
+                          int have_disp) {
+    const long long i = L.idx;
+    P.frequency[i] = L.freq;
+    P.emission_frame_energy[i] = L.emit;
+    P.x0[i] = L.s[0]; P.x1[i] = L.s[1]; P.x2[i] = L.s[2]; P.x3[i] = L.s[3];
+    P.k0[i] = L.s[4]; P.k1[i] = L.s[5]; P.k2[i] = L.s[6]; P.k3[i] = L.s[7];
+    P.I[i] = L.I[0]; P.Q[i] = L.I[1]; P.U[i] = L.I[2]; P.V[i] = L.I[3];
+    P.dlambda[i] = L.dl;
+    if (have_disp) {
+        P.theta_disp[i] = tdisp;
+        P.phi_disp[i] = pdisp;
+    }
+    P.terminate[i] = static_cast<uint8_t>(terminated);
+    P.phase[i] = static_cast<uint8_t>(L.phase);
+}
+
+// integrate_cart_ks.hpp:142-155
+template <class RHS>
+GRT_DEV void rk4_step(double s[8], double dt, const KParams& kp, int fast) {
+    double t[8];
+    t[4] = s[4];
+    const V7 k1 = RHS::eval(s, kp, fast);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + 0.5 * dt * k1.v[c];
+    const V7 k2 = RHS::eval(t, kp, fast);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + 0.5 * dt * k2.v[c];
+    const V7 k3 = RHS::eval(t, kp, fast);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + dt * k3.v[c];
+    const V7 k4 = RHS::eval(t, kp, fast);
+    const double h6 = dt / 6.0;
+#pragma unroll
+    for (int c = 0; c < 7; ++c)
+        s[sidx(c)] += h6 * (k1.v[c] + 2.0 * k2.v[c] + 2.0 * k3.v[c] + k4.v[c]);
+}
+
+// One Fehlberg attempt (integrate_cart_ks.hpp:159-227); returns 1 if accepted
+// (s advanced), 0 if rejected; *dl receives the next proposed step either way.
+template <class RHS>
+GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, const V7& k1, int fast) {
+    const double dt = *dl;
+    double t[8];
+    t[4] = s[4];
+#pragma unroll
+    for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + dt * a21 * k1.v[c];
+    const V7 k2 = RHS::eval(t, kp, fast);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + dt * (a31 * k1.v[c] + a32 * k2.v[c]);
+    const V7 k3 = RHS::eval(t, kp, fast);
+#pragma unroll
+    for (int c = 0; c < 7; ++c)
+        t[sidx(c)] = s[sidx(c)] + dt * (a41 * k1.v[c] + a42 * k2.v[c] + a43 * k3.v[c]);
+    const V7 k4 = RHS::eval(t, kp, fast);
+#pragma unroll
+    for (int c = 0; c < 7; ++c)
+        t[sidx(c)] = s[sidx(c)] + dt * (a51 * k1.v[c] + a52 * k2.v[c] + a53 * k3.v[c] + a54 * k4.v[c]);
+    const V7 k5 = RHS::eval(t, kp, fast);
+#pragma unroll
+    for (int c = 0; c < 7; ++c)
+        t[sidx(c)] = s[sidx(c)] + dt * (a61 * k1.v[c] + a62 * k2.v[c] + a63 * k3.v[c] +
+                                        a64 * k4.v[c] + a65 * k5.v[c]);
+    const V7 k6 = RHS::eval(t, kp, fast);
+    double x5[7];
+    double err = 0.0;
+    bool finite = isfinite(s[4]);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) {
+        const double si = s[sidx(c)];
+        const double x4 = si + dt * (b41 * k1.v[c] + b43 * k3.v[c] + b44 * k4.v[c] + b45 * k5.v[c]);
+        x5[c] = si + dt * (b51 * k1.v[c] + b53 * k3.v[c] + b54 * k4.v[c] + b55 * k5.v[c] + b56 * k6.v[c]);
+        const double sc = kp.atol + kp.rtol * fmax(fabs(x5[c]), fabs(x4));
+        const double ratio = fabs(x5[c] - x4) / sc;
+        if (!isfinite(x5[c]) || !isfinite(ratio)) finite = false;
+        err = fmax(err, ratio);
+    }
+    if (!finite) {
+        *dl = dt * kp.min_scale;
+        return 0;
+    }
+    if (err == 0.0) {
+        *dl = dt * kp.max_scale;
+#pragma unroll
+        for (int c = 0; c < 7; ++c) s[sidx(c)] = x5[c];
+        return 1;
+    }
+    // pow(1/err, 0.25) of the reference, correctly rounded (see grt_fourth_root.cuh)
+    double scale = kp.safety * fourth_root_cr(1.0 / err);
+    scale = fmin(kp.max_scale, fmax(kp.min_scale, scale));
+    *dl = dt * scale;
+    if (err <= 1.0) {
+#pragma unroll
+        for (int c = 0; c < 7; ++c) s[sidx(c)] = x5[c];
+        return 1;
+    }
+    return 0;
+}
+
+struct LaneCounters {
+    unsigned long long terminated, accepted, rejected, calls, max_term_step;
+};
+
+// Everything after the integration step of one call (integrate_cart_ks.hpp:307-417).
+// phase0 is the phase loaded at the start of the call.  Returns 1 if the photon
+// terminated.
+GRT_DEV int post_step(const KParams& kp, const double* s_r, const double* s_th, const double* s_ph,
+                      Lane& L, int phase0, double taken, int64_t step, double& tdisp, double& pdisp,
+                      int& have_disp) {
+    L.radius = ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
+    L.have_radius = 1;
+    const bool backward = phase0 == 1;  // ImageBackward
+    const bool needs = kp.scat_on || kp.abs_on || kp.emis_on || (kp.image_mode && backward);
+    FluidSample fs;
+    const bool sampled = needs && sample_fluid(kp, s_r, s_th, s_ph, L.s, L.radius, fs);
+    int terminated = 0;
+    if (kp.image_mode && backward && sampled) {
+        Philox rng(kp.seed, L.id, static_cast<uint32_t>(step));
+        double nu = 0.0, E = 0.0;
+        bool generated = false;
+        const double dcode = fs.fluid.density_g_cm3 / kp.density_scale;
+        const int packets = ComputeSuperphotonsPerCell(dcode, kp.norm);
+        if (packets > 0 && kp.generator == 0) {
+            generated = generate_blackbody(fs.fluid, rng, packets, kp.energy, nu, E);
+        } else if (packets > 0 && kp.generator == 1) {
+            generated = generate_power_law(rng, packets, kp.pl_slope, kp.nu_min, kp.nu_max, kp.energy, nu, E);
+        } else if (packets > 0) {
+            generated = GeneratePhotonsCustom(fs.fluid, rng, packets, kp.nu_custom, kp.energy, nu, E);
+        }
+        if (generated) {
+            L.freq = nu;
+            double ee = 0.0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) ee -= L.s[4 + c] * fs.e[0][c];
+            L.emit = ee;
+            L.I[0] = E;
+            L.I[1] = L.I[2] = L.I[3] = 0.0;
+            L.dl = -fabs(L.dl);
+            L.phase = 2;  // ImageForward
+        } else {
+            L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+            L.phase = 4;  // Rejected
+            terminated = 1;
+        }
+    } else if (sampled && !backward) {
+        if (kp.abs_on) {
+            double dtau = ComputeOpticalDepthIncrement(fs.fluid, L.freq, taken, kp.kappa);
+            if (kp.m_abs) dtau = kp.m_abs[fs.cell] * dtau;
+            const double att = exp(-dtau);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) L.I[q] *= att;
+        }
+        if (kp.emis_on) {
+            double dI = ComputeEmissivityIncrement(fs.fluid, L.freq, taken, kp.jcoef);
+            if (kp.m_emis) dI = kp.m_emis[fs.cell] * dI;
+            L.I[0] += dI;
+        }
+        if (kp.scat_on) {
+            Philox rng(kp.seed, L.id, static_cast<uint32_t>(step));
+            maybe_scatter(L.s, L.I, kp.albedo, fabs(L.dl), kp.length_scale, fs, kp.a, kp.M, rng);
+        }
+    }
+    if (kp.image_mode && phase0 == 2) {  // ImageForward
+        double u = 0.0, v = 0.0;
+        const int crossing = camera_crossing(kp, L.s, u, v);
+        if (crossing > 0) {
+            const double eo = camera_observer_energy(kp, L.s);
+            const double ee = L.emit;
+            if (eo > 0.0 && ee > 0.0 && isfinite(eo) && isfinite(ee)) {
+                L.freq *= eo / ee;
+            } else {
+                L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+            }
+            tdisp = u;
+            pdisp = v;
+            have_disp = 1;
+            L.phase = 3;  // ImageArrived
+            terminated = 1;
+        } else if (crossing < 0) {
+            L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+            L.phase = 4;
+            terminated = 1;
+        }
+    }
+    return terminated;
+}
+
+template <int INTEGRATOR, class RHS>
+GRT_DEV void trace_body(const KParams& kp, const double* s_r, const double* s_th, const double* s_ph) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    Lane L;
+    L.idx = -1;
+    LaneCounters cnt = {0, 0, 0, 0, 0};
+    bool exhausted = false;
+    unsigned long long local_next = 0, local_end = 0;
+    unsigned long long iters = 0;
+    bool timed_out = false;
+    double tdisp = 0.0, pdisp = 0.0;
+    int have_disp = 0;
+
+    while (true) {
+        // ---- refill idle lanes from the warp's block / the global queue ----
+        const unsigned idle = __ballot_sync(kFull, L.idx < 0);
+        if (idle && !(exhausted && local_next >= local_end)) {
+            const int nidle = __popc(idle);
+            if (nidle >= kp.refill_threshold || idle == kFull) {
+                unsigned long long base_a = local_next;
+                unsigned long long take_a = local_end - local_next;
+                if (take_a > static_cast<unsigned long long>(nidle)) take_a = nidle;
+                local_next += take_a;
+                unsigned long long base_b = 0, take_b = 0;
+                if (take_a < static_cast<unsigned long long>(nidle) && !exhausted) {
+                    unsigned long long claim = 0;
+                    if (lane == 0) claim = atomicAdd(&kp.counters->queue_head,
+                                                     static_cast<unsigned long long>(kp.grab));
+                    claim = __shfl_sync(kFull, claim, 0);
+                    if (claim >= kp.n) {
+                        exhausted = true;
+                    } else {
+                        local_next = claim;
+                        local_end = claim + kp.grab < kp.n ? claim + kp.grab : kp.n;
+                        take_b = local_end - local_next;
+                        const unsigned long long want = nidle - take_a;
+                        if (take_b > want) take_b = want;
+                        base_b = local_next;
+                        local_next += take_b;
+                    }
+                }
+                if (L.idx < 0) {
+                    const unsigned long long rank = __popc(idle & lt_mask);
+                    long long q = -1;
+                    if (rank < take_a) q = static_cast<long long>(base_a + rank);
+                    else if (rank - take_a < take_b) q = static_cast<long long>(base_b + (rank - take_a));
+                    if (q >= 0 && !kp.ph.terminate[q]) {
+                        load_photon(kp.ph, q, L);
+                        L.idx = q;
+                        have_disp = 0;
+                    }
+                }
+            }
+        }
+        const unsigned active = __ballot_sync(kFull, L.idx >= 0);
+        if (!active) {
+            if (exhausted && local_next >= local_end) break;
+            continue;
+        }
+        if (++iters > kp.max_iterations) {
+            timed_out = true;
+            break;
+        }
+        if (L.idx < 0) continue;
+
+        // ---- one unit of work for this lane ----
+        int finished = 0, terminated = 0;
+        if (!L.mid_call) {
+            if (L.calls >= kp.budget) {
+                finished = 1;  // budget of this launch used; photon stays live
+            } else {
+                ++L.calls;
+                ++cnt.calls;
+                const double r = L.have_radius ? L.radius : ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
+                if (r <= kp.r_min) {
+                    L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+                    L.phase = 4;
+                    finished = terminated = 1;
+                } else if (r > kp.r_max) {
+                    L.phase = 4;
+                    finished = terminated = 1;
+                } else if (INTEGRATOR == 0) {
+                    const int phase0 = L.phase;
+                    const double taken = L.dl;
+                    rk4_step<RHS>(L.s, taken, kp, 1);
+                    RHS::after_accept(L.s, kp, 1);
+                    ++cnt.accepted;
+                    terminated = post_step(kp, s_r, s_th, s_ph, L, phase0, taken,
+                                           kp.step0 + L.calls - 1, tdisp, pdisp, have_disp);
+                    finished = terminated;
+                } else {
+                    // Mixed form: an RK45 call may use the FP32 right-hand side only
+                    // when its step sequence cannot change which fluid cell the ray
+                    // samples next: after emission (not ImageBackward) and outside
+                    // the fluid grid.  Fixed-step RK4 calls may use it everywhere.
+                    L.fast = (L.phase != 1 && r * r > kp.fp32_min_radius_sq) ? 1 : 0;
+                    L.k1 = RHS::eval(L.s, kp, L.fast);
+                    L.dl_try = L.dl;
+                    L.attempts = 0;
+                    L.mid_call = 1;
+                }
+            }
+        }
+        if (INTEGRATOR == 1 && L.mid_call) {
+            const double taken = L.dl_try;
+            const int ok = rk45_attempt<RHS>(kp, L.s, &L.dl_try, L.k1, L.fast);
+            ++L.attempts;
+            if (ok) {
+                RHS::after_accept(L.s, kp, L.fast);
+                ++cnt.accepted;
+                L.dl = L.dl_try;
+                L.mid_call = 0;
+                const int phase0 = L.phase;
+                terminated = post_step(kp, s_r, s_th, s_ph, L, phase0, taken,
+                                       kp.step0 + L.calls - 1, tdisp, pdisp, have_disp);
+                finished = terminated;
+            } else {
+                ++cnt.rejected;
+                if (L.attempts >= 12) {
+                    L.dl = L.dl_try;
+                    L.mid_call = 0;
+                    finished = terminated = 1;  // phase and state unchanged (:294-297)
+                }
+            }
+        }
+        if (finished) {
+            store_photon(kp.ph, L, terminated, tdisp, pdisp, have_disp);
+            if (terminated) {
+                ++cnt.terminated;
+                const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
+                if (ts > cnt.max_term_step) cnt.max_term_step = ts;
+            }
+            L.idx = -1;
+        }
+    }
+    if (timed_out) {
+        // Leave every photon consistent: write back what this lane holds.
+        if (L.idx >= 0) store_photon(kp.ph, L, 0, tdisp, pdisp, have_disp);
+        if (lane == 0) atomicAdd(&kp.counters->timed_out, 1ull);
+    }
+    // ---- flush counters: warp reduce, one atomic per counter per warp ----
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        cnt.terminated += __shfl_down_sync(kFull, cnt.terminated, off);
+        cnt.accepted += __shfl_down_sync(kFull, cnt.accepted, off);
+        cnt.rejected += __shfl_down_sync(kFull, cnt.rejected, off);
+        cnt.calls += __shfl_down_sync(kFull, cnt.calls, off);
+        const unsigned long long m = __shfl_down_sync(kFull, cnt.max_term_step, off);
+        if (m > cnt.max_term_step) cnt.max_term_step = m;
+    }
+    if (lane == 0) {
+        if (cnt.terminated) atomicAdd(&kp.counters->terminated, cnt.terminated);
+        if (cnt.accepted) atomicAdd(&kp.counters->accepted, cnt.accepted);
+        if (cnt.rejected) atomicAdd(&kp.counters->rejected, cnt.rejected);
+        if (cnt.calls) atomicAdd(&kp.counters->calls, cnt.calls);
+        if (cnt.max_term_step) atomicMax(&kp.counters->max_term_step, cnt.max_term_step);
+    }
+}
+
+// Stage the separable axes into shared memory (the lookup reads them every step).
+GRT_DEV void stage_axes(const KParams& kp, double* smem, const double*& s_r, const double*& s_th,
+                        const double*& s_ph) {
+    const KGrid& G = kp.grid;
+    if (G.available && G.separable) {
+        double* r = smem;
+        double* th = r + G.nr;
+        double* ph = th + G.nth;
+        for (int q = threadIdx.x; q < G.nr; q += blockDim.x) r[q] = G.r_axis[q];
+        for (int q = threadIdx.x; q < G.nth; q += blockDim.x) th[q] = G.th_axis[q];
+        for (int q = threadIdx.x; q < G.nph; q += blockDim.x) ph[q] = G.ph_axis[q];
+        s_r = r;
+        s_th = th;
+        s_ph = ph;
+    } else {
+        s_r = s_th = s_ph = nullptr;
+    }
+    __syncthreads();
+}
+
+}  // namespace dev
+}  // namespace grt

@@ -1,0 +1,59 @@
+"""Launch-shape autotuner for the persistent trace kernel.
+
+Searches threads per block, resident blocks per SM, the per-warp refill
+threshold (idle lanes before a warp pulls new photons) and the photons a warp
+claims per queue access, timing each candidate with the library's own CUDA
+events around the trace launch on the actual workload.  Results are cached per
+(workload key, precision, integrator) for the life of the process.
+"""
+
+from __future__ import annotations
+
+import itertools
+
+_CACHE: dict = {}
+
+THREADS = (64, 128, 256)
+REFILL = (1, 4, 8, 16, 32)
+GRAB = (32, 64, 256)
+
+
+def candidates(occupancy_threads: int = 256):
+    """Launch shapes with the same resident threads per SM (the kernel's
+    register footprint fixes occupancy), crossed with the queue knobs."""
+    for tpb, refill, grab in itertools.product(THREADS, REFILL, GRAB):
+        yield dict(threads_per_block=tpb, blocks_per_sm=max(1, occupancy_threads // tpb),
+                   refill_threshold=refill, photons_per_grab=grab)
+
+
+def tune(ctx, prepare, key, reps: int = 2, occupancy_threads: int = 256, log=None):
+    """Pick the fastest launch shape for `ctx`.
+
+    prepare(ctx) must reset the photons (e.g. re-initialise the pixel grid);
+    each candidate is run `reps` times after one warm-up and scored by its
+    best trace-kernel time.  Returns (best_config, best_ms, table).
+    """
+    k = (key, ctx.params.precision, ctx.params.integrator)
+    if k in _CACHE:
+        cfg, ms, table = _CACHE[k]
+        ctx.set_launch_config(**cfg)
+        return cfg, ms, table
+    table = []
+    best = None
+    for cfg in candidates(occupancy_threads):
+        ctx.set_launch_config(**cfg)
+        prepare(ctx)
+        ctx.run()
+        t = []
+        for _ in range(reps):
+            prepare(ctx)
+            t.append(ctx.run()["trace_ms"])
+        ms = min(t)
+        table.append((cfg, ms))
+        if log:
+            log(f"autotune {key} {cfg} {ms:.3f} ms")
+        if best is None or ms < best[1]:
+            best = (cfg, ms)
+    ctx.set_launch_config(**best[0])
+    _CACHE[k] = (best[0], best[1], table)
+    return best[0], best[1], table

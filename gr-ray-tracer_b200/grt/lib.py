@@ -1,0 +1,227 @@
+"""ctypes binding of lib/libgrt_b200.so (the C ABI declared in include/grt.h).
+
+The product path is: Python (or any C caller) -> C ABI -> sm_100a kernels.
+Nothing here computes physics; if the shared library is missing the import
+fails loudly instead of falling back to anything else.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from .abi import (GRT_OK, STATUS_NAMES, ImageProducts, LaunchConfig, Params, PhotonArrays, PhotonSoA,
+                  ProductArrays, RunStats)
+
+PKG_ROOT = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG_ROOT / "lib" / "libgrt_b200.so"
+
+
+class GrtError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def build(jobs: int = 4) -> Path:
+    """Compile the CUDA library for sm_100a (nvcc; no GPU needed)."""
+    subprocess.run(["make", "-s", "-j", str(jobs), "-C", str(PKG_ROOT)], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def load(path: Path | None = None):
+    """Load the shared library once and declare every entry point of grt.h."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(path or os.environ.get("GRT_LIB", LIB_PATH))
+    if not path.exists():
+        raise FileNotFoundError(f"{path} is not built; run grt.lib.build() (nvcc, sm_100a)")
+    L = C.CDLL(str(path))
+    vp = C.c_void_p
+    P = C.POINTER
+    L.grt_abi_version.restype = C.c_int32
+    L.grt_build_info.restype = C.c_char_p
+    L.grt_params_default.argtypes = [P(Params)]
+    L.grt_params_default.restype = None
+    L.grt_params_validate.argtypes = [P(Params), C.c_char_p, C.c_size_t]
+    L.grt_params_from_toml.argtypes = [C.c_char_p, P(Params), C.c_char_p, C.c_size_t, C.c_char_p,
+                                       C.c_size_t, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]
+    L.grt_create.argtypes = [P(Params), P(vp)]
+    L.grt_destroy.argtypes = [vp]
+    L.grt_destroy.restype = None
+    L.grt_last_error.argtypes = [vp]
+    L.grt_last_error.restype = C.c_char_p
+    L.grt_set_params.argtypes = [vp, P(Params)]
+    L.grt_set_stream.argtypes = [vp, vp]
+    L.grt_synchronize.argtypes = [vp]
+    L.grt_upload_grid.argtypes = [vp, C.c_size_t, C.c_size_t, C.c_size_t] + [P(C.c_double)] * 7
+    L.grt_upload_grid_numpy_dir.argtypes = [vp, C.c_char_p]
+    L.grt_upload_photons.argtypes = [vp, P(PhotonSoA), C.c_size_t]
+    L.grt_init_image_photons.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint64]
+    L.grt_run.argtypes = [vp, P(RunStats)]
+    L.grt_download_photons.argtypes = [vp, P(PhotonSoA)]
+    L.grt_photon_count.argtypes = [vp]
+    L.grt_photon_count.restype = C.c_size_t
+    L.grt_get_image_products.argtypes = [vp, P(ImageProducts)]
+    L.grt_write_image_products_npz.argtypes = [vp, C.c_char_p, C.c_char_p]
+    L.grt_get_launch_config.argtypes = [vp, P(LaunchConfig)]
+    L.grt_set_launch_config.argtypes = [vp, P(LaunchConfig)]
+    L.grt_measure_fma_peaks.argtypes = [P(C.c_double), P(C.c_double)]
+    for name in ("grt_measure_fma_peaks", "grt_params_validate", "grt_params_from_toml", "grt_create", "grt_set_params",
+                 "grt_set_stream", "grt_synchronize", "grt_upload_grid", "grt_upload_grid_numpy_dir",
+                 "grt_upload_photons", "grt_init_image_photons", "grt_run", "grt_download_photons",
+                 "grt_get_image_products", "grt_write_image_products_npz", "grt_get_launch_config",
+                 "grt_set_launch_config"):
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def default_params() -> Params:
+    p = Params()
+    load().grt_params_default(C.byref(p))
+    return p
+
+
+def validate_params(p: Params):
+    buf = C.create_string_buffer(512)
+    rc = load().grt_params_validate(C.byref(p), buf, 512)
+    if rc != GRT_OK:
+        raise GrtError(rc, buf.value.decode())
+
+
+def params_from_toml(path):
+    """Parse a reference TOML file: returns (Params, numpy_dir, output_dir, name)."""
+    L = load()
+    p = Params()
+    bufs = [C.create_string_buffer(4096) for _ in range(4)]
+    rc = L.grt_params_from_toml(str(path).encode(), C.byref(p), bufs[0], 4096, bufs[1], 4096, bufs[2], 4096,
+                                bufs[3], 4096)
+    if rc != GRT_OK:
+        raise GrtError(rc, bufs[3].value.decode())
+    return p, bufs[0].value.decode(), bufs[1].value.decode(), bufs[2].value.decode()
+
+
+def measure_fma_peaks():
+    """(fp64, fp32) FMA throughput of the current device in TFLOP/s."""
+    d, f = C.c_double(), C.c_double()
+    rc = load().grt_measure_fma_peaks(C.byref(d), C.byref(f))
+    if rc != GRT_OK:
+        raise GrtError(rc, "grt_measure_fma_peaks failed")
+    return d.value, f.value
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Context:
+    """One device context of the hot path (owns every device buffer)."""
+
+    def __init__(self, params: Params):
+        self.lib = load()
+        self._h = C.c_void_p()
+        self.params = params.copy()
+        rc = self.lib.grt_create(C.byref(self.params), C.byref(self._h))
+        if rc != GRT_OK:
+            raise GrtError(rc, "grt_create failed (needs an sm_100 device and valid params)")
+
+    def close(self):
+        if self._h:
+            self.lib.grt_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc != GRT_OK:
+            raise GrtError(rc, self.lib.grt_last_error(self._h).decode())
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_params(self, p: Params):
+        self.params = p.copy()
+        self._check(self.lib.grt_set_params(self._h, C.byref(self.params)))
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self.lib.grt_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def synchronize(self):
+        self._check(self.lib.grt_synchronize(self._h))
+
+    def upload_grid(self, grid: dict | None):
+        """grid: dict of the seven .npy arrays (name -> ndarray), or None for no fluid."""
+        if grid is None:
+            self._check(self.lib.grt_upload_grid(self._h, 0, 0, 0, *([None] * 7)))
+            return
+        keys = ("r.npy", "theta.npy", "phi.npy", "rho.npy", "Tgas.npy", "vel.npy", "mag.npy")
+        arrs = [np.ascontiguousarray(grid[k], dtype=np.float64) for k in keys]
+        nr, nth, nph = arrs[0].shape
+        self._check(self.lib.grt_upload_grid(self._h, nr, nth, nph, *[_dp(a) for a in arrs]))
+
+    def upload_grid_numpy_dir(self, path):
+        self._check(self.lib.grt_upload_grid_numpy_dir(self._h, str(path).encode()))
+
+    def upload_photons(self, ph: PhotonArrays):
+        soa = ph.soa()
+        self._check(self.lib.grt_upload_photons(self._h, C.byref(soa), ph.n))
+
+    def init_image_photons(self, nx, ny, id_offset=0):
+        self._check(self.lib.grt_init_image_photons(self._h, nx, ny, id_offset))
+
+    def run(self) -> dict:
+        st = RunStats()
+        rc = self.lib.grt_run(self._h, C.byref(st))
+        self._check(rc)
+        return st.as_dict()
+
+    @property
+    def n(self):
+        return int(self.lib.grt_photon_count(self._h))
+
+    def download_photons(self, out: PhotonArrays | None = None) -> PhotonArrays:
+        out = out or PhotonArrays(self.n)
+        soa = out.soa()
+        self._check(self.lib.grt_download_photons(self._h, C.byref(soa)))
+        return out
+
+    def image_products(self, out: ProductArrays | None = None) -> ProductArrays:
+        out = out or ProductArrays.for_params(self.params)
+        s = out.struct()
+        self._check(self.lib.grt_get_image_products(self._h, C.byref(s)))
+        return out
+
+    def write_image_products_npz(self, output_dir, name):
+        self._check(self.lib.grt_write_image_products_npz(self._h, str(output_dir).encode(), name.encode()))
+
+    def launch_config(self) -> dict:
+        lc = LaunchConfig()
+        self._check(self.lib.grt_get_launch_config(self._h, C.byref(lc)))
+        return lc.as_dict()
+
+    def set_launch_config(self, **kw):
+        lc = LaunchConfig()
+        self._check(self.lib.grt_get_launch_config(self._h, C.byref(lc)))
+        for k, v in kw.items():
+            setattr(lc, k, int(v))
+        self._check(self.lib.grt_set_launch_config(self._h, C.byref(lc)))

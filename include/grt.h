@@ -251,6 +251,13 @@ grt_status grt_write_image_products_npz(grt_ctx* ctx, const char* output_dir, co
 grt_status grt_get_launch_config(const grt_ctx* ctx, grt_launch_config* cfg);
 grt_status grt_set_launch_config(grt_ctx* ctx, const grt_launch_config* cfg);
 
+/*
+ * Roofline denominators (no counterpart in the reference): FP64 and FP32 FMA
+ * throughput of the current device in TFLOP/s (2 flops per FMA), measured
+ * with CUDA events over long independent FMA chains.
+ */
+grt_status grt_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops);
+
 #ifdef __cplusplus
 }
 #endif

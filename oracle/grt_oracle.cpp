@@ -27,6 +27,92 @@
 namespace oracle {
 
 using real = double;
+
+// How the RK45 controller evaluates pow(1/err, 0.25):
+//   0 = correctly rounded fourth root (what the sm_100a kernels compute);
+//   1 = std::pow, i.e. glibc, exactly like the reference's host build.
+int g_pow_mode = 0;
+
+// Correctly rounded x^(1/4), written independently of the kernel's version:
+// start from sqrt(sqrt(x)) and step while x lies beyond the fourth power of a
+// rounding midpoint, compared exactly with 32-bit limbs.
+namespace cr {
+using limbs = std::vector<uint64_t>;  // base 2^32, little endian
+limbs from_u64(uint64_t v) { return {v & 0xffffffffu, v >> 32}; }
+limbs mul(const limbs& a, const limbs& b) {
+    limbs r(a.size() + b.size() + 1, 0);
+    for (size_t i = 0; i < a.size(); ++i) {
+        uint64_t carry = 0;
+        for (size_t j = 0; j < b.size(); ++j) {
+            const uint64_t t = r[i + j] + a[i] * b[j] + carry;
+            r[i + j] = t & 0xffffffffu;
+            carry = t >> 32;
+        }
+        size_t k = i + b.size();
+        while (carry) {
+            const uint64_t t = r[k] + carry;
+            r[k] = t & 0xffffffffu;
+            carry = t >> 32;
+            ++k;
+        }
+    }
+    return r;
+}
+limbs shl(uint64_t v, int s) {  // v * 2^s
+    limbs r(static_cast<size_t>(s / 32 + 4), 0);
+    const int w = s / 32, b = s % 32;
+    const unsigned __int128 x = static_cast<unsigned __int128>(v) << b;
+    for (int q = 0; q < 3; ++q) r[w + q] = static_cast<uint64_t>(x >> (32 * q)) & 0xffffffffu;
+    return r;
+}
+int cmp(limbs a, limbs b) {
+    while (a.size() < b.size()) a.push_back(0);
+    while (b.size() < a.size()) b.push_back(0);
+    for (size_t k = a.size(); k-- > 0;)
+        if (a[k] != b[k]) return a[k] > b[k] ? 1 : -1;
+    return 0;
+}
+void split(double v, uint64_t& m, int& e) {
+    int ex;
+    const double f = std::frexp(v, &ex);  // v = f 2^ex, f in [0.5, 1)
+    m = static_cast<uint64_t>(std::ldexp(f, 53));
+    e = ex - 53;
+    while (m && !(m & 1)) { m >>= 1; ++e; }
+}
+// sign of A^4 2^(4 ea) - X 2^ex
+int cmp_mid4(uint64_t A, int ea, uint64_t X, int ex) {
+    const limbs a = from_u64(A);
+    const limbs p = mul(mul(a, a), mul(a, a));
+    const int s = ex - 4 * ea;
+    if (s >= 0) return cmp(p, shl(X, s));
+    return cmp(mul(p, shl(1, -s)), from_u64(X));
+}
+double fourth_root(double x) {
+    if (!(x > 0.0) || !std::isfinite(x)) return std::sqrt(std::sqrt(x));
+    double y = std::sqrt(std::sqrt(x));
+    uint64_t X;
+    int ex;
+    split(x, X, ex);
+    for (int it = 0; it < 4; ++it) {
+        const double up = std::nextafter(y, INFINITY), dn = std::nextafter(y, 0.0);
+        // midpoints as odd integers times powers of two
+        uint64_t Mu; int eu; split(y + 0.0, Mu, eu);
+        const double hi_gap = up - y, lo_gap = y - dn;
+        int eg; uint64_t g;
+        split(hi_gap, g, eg);  // gap is a power of two: g == 1
+        // y = Mu 2^eu; mid_up = y + gap/2 = (Mu 2^(eu-eg+1) + 1) 2^(eg-1)
+        const uint64_t Aup = (Mu << (eu - eg + 1)) + 1;
+        if (cmp_mid4(Aup, eg - 1, X, ex) < 0) { y = up; continue; }
+        split(lo_gap, g, eg);
+        const uint64_t Adn = (Mu << (eu - eg + 1)) - 1;
+        if (cmp_mid4(Adn, eg - 1, X, ex) > 0) { y = dn; continue; }
+        break;
+    }
+    return y;
+}
+}  // namespace cr
+
+real controller_root(real x) { return g_pow_mode == 1 ? std::pow(x, real(0.25)) : cr::fourth_root(x); }
 using grt::FluidCellCGS;
 
 constexpr real PI = 3.14159265358979323846;  // src/utils.hpp:16
@@ -677,7 +763,7 @@ struct Stepper {
             for (int i = 0; i < 8; ++i) s[i] = x5[i];
             return 1;
         }
-        real scale = p->safety * std::pow(real(1.0) / err, real(0.25));
+        real scale = p->safety * controller_root(real(1.0) / err);
         scale = std::fmin(p->max_step_scale, std::fmax(p->min_step_scale, scale));
         if (err <= 1.0) {
             *dlambda = dt * scale;
@@ -898,6 +984,148 @@ size_t observation_bin(real value, real lo, real hi, size_t bins) {
 
 }  // namespace oracle
 
+
+// ---------------------------------------------------------------------------
+// Op counting: the RHS and the RK4 / RKF45 stage arithmetic above, written
+// once more over a scalar type that counts +, -, *, / and sqrt (and pow, as
+// one op), in the same source order, to pin the algorithmic FLOP counts the
+// roofline uses.  A test checks that the Counted instantiation produces the
+// same values as the double code above.
+// ---------------------------------------------------------------------------
+namespace opcount {
+struct Counter { uint64_t add = 0, mul = 0, div = 0, sqrt = 0, pow = 0; };
+Counter g;
+struct N {
+    double v;
+    N(double x = 0.0) : v(x) {}
+};
+inline N operator+(N a, N b) { ++g.add; return N(a.v + b.v); }
+inline N operator-(N a, N b) { ++g.add; return N(a.v - b.v); }
+inline N operator*(N a, N b) { ++g.mul; return N(a.v * b.v); }
+inline N operator/(N a, N b) { ++g.div; return N(a.v / b.v); }
+inline N operator-(N a) { return N(-a.v); }
+inline N& operator+=(N& a, N b) { a = a + b; return a; }
+inline bool operator<(N a, N b) { return a.v < b.v; }
+inline bool operator>(N a, N b) { return a.v > b.v; }
+inline bool operator<=(N a, N b) { return a.v <= b.v; }
+inline bool operator==(N a, N b) { return a.v == b.v; }
+inline N Sqrt(N a) { ++g.sqrt; return N(std::sqrt(a.v)); }
+inline N Fabs(N a) { return N(std::fabs(a.v)); }
+inline N Fmax(N a, N b) { return N(std::fmax(a.v, b.v)); }
+inline N Fmin(N a, N b) { return N(std::fmin(a.v, b.v)); }
+inline N Pow(N a, N b) { ++g.pow; return N(std::pow(a.v, b.v)); }
+inline bool Isfinite(N a) { return std::isfinite(a.v); }
+template <class T> T SQ(T x) { return x * x; }
+template <class T> T CU(T x) { return x * x * x; }
+template <class T> T QU(T x) { return x * x * x * x; }
+
+// kerr_schild_core.hpp:157-192 with :36-46, :58-77, :85-95
+template <class T>
+void rhs(const T X[4], const T p[4], T a, T M, T out[8]) {
+    const T rsq = SQ(X[1]) + SQ(X[2]) + SQ(X[3]);
+    const T A = rsq - SQ(a);
+    const T S = Sqrt(SQ(A) + T(4.0) * SQ(a * X[3]));
+    const T r = Sqrt(T(0.5) * (A + S));
+    const T opas = T(1.0) + A / S;
+    T dr[3];
+    dr[0] = X[1] * opas / (T(2.0) * r);
+    dr[1] = X[2] * opas / (T(2.0) * r);
+    dr[2] = (X[3] * opas + T(2.0) * SQ(a) * X[3] / S) / (T(2.0) * r);
+    const T B = SQ(r) + SQ(a);
+    T l[4], dl[3][4];
+    l[0] = T(1.0);
+    l[1] = (r * X[1] + a * X[2]) / B;
+    l[2] = (r * X[2] - a * X[1]) / B;
+    l[3] = X[3] / r;
+    for (int k = 0; k < 3; ++k) {
+        const T dx = T(k == 0 ? 1.0 : 0.0), dy = T(k == 1 ? 1.0 : 0.0), dz = T(k == 2 ? 1.0 : 0.0);
+        const T dB = T(2.0) * r * dr[k];
+        dl[k][0] = T(0.0);
+        dl[k][1] = ((dr[k] * X[1] + r * dx) + a * dy - l[1] * dB) / B;
+        dl[k][2] = ((dr[k] * X[2] + r * dy) - a * dx - l[2] * dB) / B;
+        dl[k][3] = (dz - l[3] * dr[k]) / r;
+    }
+    const T D = QU(r) + SQ(a * X[3]);
+    const T H = M * CU(r) / D;
+    T dH[3];
+    for (int k = 0; k < 3; ++k) {
+        const T dz = T(k == 2 ? 1.0 : 0.0);
+        const T dD = T(4.0) * CU(r) * dr[k] + T(2.0) * SQ(a) * X[3] * dz;
+        dH[k] = M * (T(3.0) * SQ(r) * dr[k] * D - CU(r) * dD) / SQ(D);
+    }
+    const T lup[4] = {-l[0], l[1], l[2], l[3]};
+    T ldp = T(0.0);
+    for (int mu = 0; mu < 4; ++mu) ldp += lup[mu] * p[mu];
+    out[0] = -p[0] - T(2.0) * H * lup[0] * ldp;
+    for (int mu = 1; mu < 4; ++mu) out[mu] = p[mu] - T(2.0) * H * lup[mu] * ldp;
+    out[4] = T(0.0);
+    for (int k = 0; k < 3; ++k) {
+        const T dlup[4] = {-dl[k][0], dl[k][1], dl[k][2], dl[k][3]};
+        T dldp = T(0.0);
+        for (int mu = 0; mu < 4; ++mu) dldp += dlup[mu] * p[mu];
+        out[5 + k] = dH[k] * SQ(ldp) + T(2.0) * H * ldp * dldp;
+    }
+}
+
+template <class T>
+void rhs_s(const T s[8], T a, T M, T out[8]) { rhs<T>(s, s + 4, a, M, out); }
+
+// integrate_cart_ks.hpp:142-155
+template <class T>
+void rk4(T s[8], T dt, T a, T M) {
+    T k1[8], k2[8], k3[8], k4[8], t[8];
+    rhs_s(s, a, M, k1);
+    for (int i = 0; i < 8; ++i) t[i] = s[i] + T(0.5) * dt * k1[i];
+    rhs_s(t, a, M, k2);
+    for (int i = 0; i < 8; ++i) t[i] = s[i] + T(0.5) * dt * k2[i];
+    rhs_s(t, a, M, k3);
+    for (int i = 0; i < 8; ++i) t[i] = s[i] + dt * k3[i];
+    rhs_s(t, a, M, k4);
+    for (int i = 0; i < 8; ++i) s[i] += (dt / T(6.0)) * (k1[i] + T(2.0) * k2[i] + T(2.0) * k3[i] + k4[i]);
+}
+
+// integrate_cart_ks.hpp:159-227, one attempt (k1 given); returns accepted
+template <class T>
+int rk45_attempt(T s[8], T& dl, const T k1[8], T a, T M, T atol, T rtol) {
+    const T a21 = T(1.0 / 4.0), a31 = T(3.0 / 32.0), a32 = T(9.0 / 32.0);
+    const T a41 = T(1932.0 / 2197.0), a42 = T(-7200.0 / 2197.0), a43 = T(7296.0 / 2197.0);
+    const T a51 = T(439.0 / 216.0), a52 = T(-8.0), a53 = T(3680.0 / 513.0), a54 = T(-845.0 / 4104.0);
+    const T a61 = T(-8.0 / 27.0), a62 = T(2.0), a63 = T(-3544.0 / 2565.0), a64 = T(1859.0 / 4104.0),
+            a65 = T(-11.0 / 40.0);
+    const T b41 = T(25.0 / 216.0), b43 = T(1408.0 / 2565.0), b44 = T(2197.0 / 4104.0), b45 = T(-1.0 / 5.0);
+    const T b51 = T(16.0 / 135.0), b53 = T(6656.0 / 12825.0), b54 = T(28561.0 / 56430.0), b55 = T(-9.0 / 50.0),
+            b56 = T(2.0 / 55.0);
+    const T dt = dl;
+    T k2[8], k3[8], k4[8], k5[8], k6[8], t[8];
+    for (int i = 0; i < 8; ++i) t[i] = s[i] + dt * a21 * k1[i];
+    rhs_s(t, a, M, k2);
+    for (int i = 0; i < 8; ++i) t[i] = s[i] + dt * (a31 * k1[i] + a32 * k2[i]);
+    rhs_s(t, a, M, k3);
+    for (int i = 0; i < 8; ++i) t[i] = s[i] + dt * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
+    rhs_s(t, a, M, k4);
+    for (int i = 0; i < 8; ++i) t[i] = s[i] + dt * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i] + a54 * k4[i]);
+    rhs_s(t, a, M, k5);
+    for (int i = 0; i < 8; ++i)
+        t[i] = s[i] + dt * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i] + a64 * k4[i] + a65 * k5[i]);
+    rhs_s(t, a, M, k6);
+    T x4[8], x5[8], err = T(0.0);
+    for (int i = 0; i < 8; ++i) {
+        x4[i] = s[i] + dt * (b41 * k1[i] + b43 * k3[i] + b44 * k4[i] + b45 * k5[i]);
+        x5[i] = s[i] + dt * (b51 * k1[i] + b53 * k3[i] + b54 * k4[i] + b55 * k5[i] + b56 * k6[i]);
+        const T sc = atol + rtol * Fmax(Fabs(x5[i]), Fabs(x4[i]));
+        err = Fmax(err, Fabs(x5[i] - x4[i]) / sc);
+    }
+    T scale = T(0.9) * Pow(T(1.0) / err, T(0.25));
+    scale = Fmin(T(10.0), Fmax(T(0.01), scale));
+    dl = dt * scale;
+    if (err <= T(1.0)) {
+        for (int i = 0; i < 8; ++i) s[i] = x5[i];
+        return 1;
+    }
+    return 0;
+}
+}  // namespace opcount
+
 using namespace oracle;
 
 extern "C" {
@@ -1106,6 +1334,55 @@ double oracle_philox_drand(uint64_t seed, uint64_t id, uint32_t domain, int inde
     for (int q = 0; q <= index; ++q) d = rng.drand();
     return d;
 }
+void oracle_set_pow_mode(int mode) { g_pow_mode = mode; }
+double oracle_fourth_root(double x) { return cr::fourth_root(x); }
+// Algorithmic op counts (add+sub, mul, div, sqrt, pow) of one RHS, one RK4
+// step and one RKF45 attempt (with k1 given) at the state X/P, from the
+// Counted instantiation; checks[3] = max |Counted - double| over the results.
+void oracle_op_counts(const grt_params* p, const double X[4], const double P[4], double dl,
+                      uint64_t rhs_ops[5], uint64_t rk4_ops[5], uint64_t rk45_ops[5], double checks[3]) {
+    using opcount::N;
+    auto take = [](uint64_t out[5]) {
+        const opcount::Counter c = opcount::g;
+        out[0] = c.add; out[1] = c.mul; out[2] = c.div; out[3] = c.sqrt; out[4] = c.pow;
+        opcount::g = opcount::Counter();
+    };
+    const N a(p->spin), M(p->mass);
+    N Xn[4], Pn[4], o[8];
+    for (int q = 0; q < 4; ++q) { Xn[q] = N(X[q]); Pn[q] = N(P[q]); }
+    opcount::g = opcount::Counter();
+    opcount::rhs<N>(Xn, Pn, a, M, o);
+    take(rhs_ops);
+    double od[8];
+    hamiltonian_rhs(X, P, p->spin, p->mass, od);
+    checks[0] = 0.0;
+    for (int q = 0; q < 8; ++q) checks[0] = std::fmax(checks[0], std::fabs(od[q] - o[q].v));
+    N s[8];
+    double sd[8];
+    for (int q = 0; q < 4; ++q) { s[q] = N(X[q]); s[4 + q] = N(P[q]); sd[q] = X[q]; sd[4 + q] = P[q]; }
+    opcount::rk4<N>(s, N(dl), a, M);
+    take(rk4_ops);
+    Stepper st{p, nullptr, false, false, false};
+    st.rk4(sd, dl);
+    checks[1] = 0.0;
+    for (int q = 0; q < 8; ++q) checks[1] = std::fmax(checks[1], std::fabs(sd[q] - s[q].v));
+    N k1[8], s2[8];
+    double sd2[8], kd[8];
+    for (int q = 0; q < 4; ++q) { s2[q] = N(X[q]); s2[4 + q] = N(P[q]); sd2[q] = X[q]; sd2[4 + q] = P[q]; }
+    opcount::rhs_s<N>(s2, a, M, k1);
+    opcount::g = opcount::Counter();
+    N dln(dl);
+    opcount::rk45_attempt<N>(s2, dln, k1, a, M, N(p->atol), N(p->rtol));
+    take(rk45_ops);
+    st.rhs(sd2, kd);
+    double dld = dl;
+    g_pow_mode = 1;
+    st.rk45(sd2, &dld, kd);
+    g_pow_mode = 0;
+    checks[2] = std::fabs(dld - dln.v);
+    for (int q = 0; q < 8; ++q) checks[2] = std::fmax(checks[2], std::fabs(sd2[q] - s2[q].v));
+}
+
 uint64_t oracle_observation_bin(double value, double lo, double hi, uint64_t bins) {
     return observation_bin(value, lo, hi, bins);
 }

@@ -66,8 +66,16 @@ class Oracle:
         L.oracle_philox_block.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.oracle_philox_drand.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_int]
         L.oracle_philox_drand.restype = C.c_double
+        L.oracle_set_pow_mode.argtypes = [C.c_int]
+        L.oracle_fourth_root.argtypes = [C.c_double]
+        L.oracle_fourth_root.restype = C.c_double
         L.oracle_observation_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint64]
         L.oracle_observation_bin.restype = C.c_uint64
+
+    def set_pow_mode(self, mode):
+        """'cr': correctly rounded controller root (kernel semantics);
+        'libm': std::pow like the reference's host build."""
+        self.lib.oracle_set_pow_mode({"cr": 0, "libm": 1}[mode])
 
     # ---- whole-path entry points ----
     def init_image_photons(self, p: Params, nx, ny, id_offset=0) -> PhotonArrays:
