@@ -163,7 +163,7 @@ struct Grid3 {
     }
 };
 
-GRT_DEV bool locate_general(const Grid3& g, double radius, double polar, double az, int& i, int& j,
+static __device__ __noinline__ bool locate_general(const Grid3& g, double radius, double polar, double az, int& i, int& j,
                             int& k) {
     j = g.nth / 2;
     k = g.nph / 2;
@@ -345,7 +345,7 @@ constexpr double kProtonMassCgs = 1.67262192369e-24;   // scattering.hpp:256
 constexpr double kSigmaThomsonCgs = 6.6524587158e-25;  // scattering.hpp:257
 
 // maybe_scatter_photon (scattering.hpp:259-313)
-GRT_DEV bool maybe_scatter(double s[8], double I[4], double albedo, double dl, double length_scale,
+static __device__ __noinline__ bool maybe_scatter(double s[8], double I[4], double albedo, double dl, double length_scale,
                            const FluidSample& fs, double a, double M, Philox& rng) {
     const double path_cm = dl * length_scale;
     const double ne = fs.fluid.density_g_cm3 / kProtonMassCgs;
@@ -382,7 +382,7 @@ GRT_DEV bool maybe_scatter(double s[8], double I[4], double albedo, double dl, d
 // GenerateBlackbody (photon_generation.hpp:99-124): Planck spectrum as a
 // mixture of Gamma(4, n) with weights 1/n^4; the four product draws are taken
 // in order.
-GRT_DEV bool generate_blackbody(const FluidCellCGS& cell, Philox& rng, int packets, double energy,
+static __device__ __noinline__ bool generate_blackbody(const FluidCellCGS& cell, Philox& rng, int packets, double energy,
                                 double& nu, double& E) {
     if (!(cell.temperature_k > 0.0)) return false;
     const double inverse_zeta4 = 0.9239384029215902;
@@ -403,7 +403,7 @@ GRT_DEV bool generate_blackbody(const FluidCellCGS& cell, Philox& rng, int packe
 }
 
 // GeneratePowerLaw (photon_generation.hpp:126-143)
-GRT_DEV bool generate_power_law(Philox& rng, int packets, double slope, double nu_min, double nu_max,
+static __device__ __noinline__ bool generate_power_law(Philox& rng, int packets, double slope, double nu_min, double nu_max,
                                 double energy, double& nu, double& E) {
     const double draw = rng.drand();
     if (fabs(slope - 1.0) < 1.0e-12) {

@@ -5,12 +5,16 @@
 //     eta^{mu nu} p_nu stays FP64, the Kerr-Schild correction -2H l^mu (l.p)
 //     and dp/dlambda are evaluated in FP32; being O(M/r) of the flat part,
 //     their FP32 rounding enters the trajectory at ~1e-7 M/r relative;
-//   * fast FP64 form (ks_rhs_fast): reciprocals instead of divisions, FMA.
+//   * otherwise the FP64 parity form (ks_rhs), bit-identical to the plain
+//     kernel (this translation unit is also built with -fmad=false).
 // Which one a call uses: RK4 calls (fixed step) use FP32; an RK45 call uses
 // FP32 only after emission (not ImageBackward) and outside the fluid grid.
 // Before that, the adaptive step sequence decides where the backward ray
-// first lands inside the grid -- the cell that emits it -- and FP32 noise in
-// the error estimate would move that landing point and change the image.
+// first lands inside the grid -- the cell that emits it -- and any change of
+// the step sequence, even at the last bit of FP64 (FMA contraction or a
+// reciprocal in place of a division), moves that landing point for some rays
+// and changes their emitted intensity.  After emission outside the grid the
+// Stokes vector no longer changes, so FP32 there leaves the image intact.
 //
 // Kept in FP64:
 //   * the state x^mu / p_mu and every Runge-Kutta stage combination and
@@ -39,7 +43,7 @@ struct MixedRhs {
         const double rho2 = x * x + y * y;
         const double rsq = rho2 + z * z;
         if (!fast || rsq < kp.fp64_radius_sq || rho2 < kp.fp64_axis_sin2 * rsq)
-            return to_v7(ks_rhs_fast(x, y, z, s[4], s[5], s[6], s[7], kp.a, kp.M));
+            return Fp64Rhs::eval(s, kp, 0);
         return to_v7(ks_rhs_fp32(x, y, z, rsq, s[4], s[5], s[6], s[7], kp.a, kp.M));
     }
 

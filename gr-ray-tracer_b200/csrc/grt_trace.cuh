@@ -108,61 +108,90 @@ GRT_DEV void store_photon(const KPhotons& P, const Lane& L, int terminated, doub
     P.phase[i] = static_cast<uint8_t>(L.phase);
 }
 
-// integrate_cart_ks.hpp:142-155
+// integrate_cart_ks.hpp:142-155.  One right-hand-side site inside a stage
+// loop (kept rolled: a fully unrolled step overflows the instruction cache);
+// only the running weighted sum ((k1 + 2 k2) + 2 k3) + k4 is kept, which adds
+// the stages in the reference's order.  Stage inputs s + (c dt) k with
+// c in {1/2, 1/2, 1} round exactly like the reference's s + c*dt*k.
 template <class RHS>
 GRT_DEV void rk4_step(double s[8], double dt, const KParams& kp, int fast) {
     double t[8];
+    V7 k, sum;
     t[4] = s[4];
-    const V7 k1 = RHS::eval(s, kp, fast);
+#pragma unroll 1
+    for (int st = 0; st < 4; ++st) {
+        if (st == 0) {
 #pragma unroll
-    for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + 0.5 * dt * k1.v[c];
-    const V7 k2 = RHS::eval(t, kp, fast);
+            for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)];
+        } else {
+            const double cdt = (st == 3) ? dt : 0.5 * dt;
 #pragma unroll
-    for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + 0.5 * dt * k2.v[c];
-    const V7 k3 = RHS::eval(t, kp, fast);
+            for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + cdt * k.v[c];
+        }
+        k = RHS::eval(t, kp, fast);
+        if (st == 0) {
+            sum = k;
+        } else if (st == 3) {
 #pragma unroll
-    for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + dt * k3.v[c];
-    const V7 k4 = RHS::eval(t, kp, fast);
+            for (int c = 0; c < 7; ++c) sum.v[c] = sum.v[c] + k.v[c];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 7; ++c) sum.v[c] = sum.v[c] + 2.0 * k.v[c];
+        }
+    }
     const double h6 = dt / 6.0;
 #pragma unroll
-    for (int c = 0; c < 7; ++c)
-        s[sidx(c)] += h6 * (k1.v[c] + 2.0 * k2.v[c] + 2.0 * k3.v[c] + k4.v[c]);
+    for (int c = 0; c < 7; ++c) s[sidx(c)] += h6 * sum.v[c];
 }
+
+// Stage-input rows of the Fehlberg tableau (a_{t,j}, j < t), zero padded.
+static __constant__ double kFehlbergA[5][5] = {
+    {a21, 0.0, 0.0, 0.0, 0.0},
+    {a31, a32, 0.0, 0.0, 0.0},
+    {a41, a42, a43, 0.0, 0.0},
+    {a51, a52, a53, a54, 0.0},
+    {a61, a62, a63, a64, a65}};
 
 // One Fehlberg attempt (integrate_cart_ks.hpp:159-227); returns 1 if accepted
 // (s advanced), 0 if rejected; *dl receives the next proposed step either way.
+// The five stage evaluations share one right-hand-side site in a rolled loop
+// (k1..k5 live in thread-local memory); each stage input is summed over
+// j = 1..t-1 left to right, exactly the reference's association.  For the
+// first stage, dt*(a21 k1) equals the reference's (dt*a21)*k1 because
+// a21 = 1/4 is a power of two.
 template <class RHS>
 GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, const V7& k1, int fast) {
     const double dt = *dl;
+    double kk[5][7];
+    V7 k6;
+#pragma unroll
+    for (int c = 0; c < 7; ++c) kk[0][c] = k1.v[c];
     double t[8];
     t[4] = s[4];
+#pragma unroll 1
+    for (int st = 0; st < 5; ++st) {
 #pragma unroll
-    for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + dt * a21 * k1.v[c];
-    const V7 k2 = RHS::eval(t, kp, fast);
+        for (int c = 0; c < 7; ++c) {
+            double acc = kFehlbergA[st][0] * kk[0][c];
+            for (int j = 1; j <= st; ++j) acc = acc + kFehlbergA[st][j] * kk[j][c];
+            t[sidx(c)] = s[sidx(c)] + dt * acc;
+        }
+        const V7 k = RHS::eval(t, kp, fast);
+        if (st < 4) {
 #pragma unroll
-    for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + dt * (a31 * k1.v[c] + a32 * k2.v[c]);
-    const V7 k3 = RHS::eval(t, kp, fast);
-#pragma unroll
-    for (int c = 0; c < 7; ++c)
-        t[sidx(c)] = s[sidx(c)] + dt * (a41 * k1.v[c] + a42 * k2.v[c] + a43 * k3.v[c]);
-    const V7 k4 = RHS::eval(t, kp, fast);
-#pragma unroll
-    for (int c = 0; c < 7; ++c)
-        t[sidx(c)] = s[sidx(c)] + dt * (a51 * k1.v[c] + a52 * k2.v[c] + a53 * k3.v[c] + a54 * k4.v[c]);
-    const V7 k5 = RHS::eval(t, kp, fast);
-#pragma unroll
-    for (int c = 0; c < 7; ++c)
-        t[sidx(c)] = s[sidx(c)] + dt * (a61 * k1.v[c] + a62 * k2.v[c] + a63 * k3.v[c] +
-                                        a64 * k4.v[c] + a65 * k5.v[c]);
-    const V7 k6 = RHS::eval(t, kp, fast);
+            for (int c = 0; c < 7; ++c) kk[st + 1][c] = k.v[c];
+        } else {
+            k6 = k;
+        }
+    }
     double x5[7];
     double err = 0.0;
     bool finite = isfinite(s[4]);
 #pragma unroll
     for (int c = 0; c < 7; ++c) {
         const double si = s[sidx(c)];
-        const double x4 = si + dt * (b41 * k1.v[c] + b43 * k3.v[c] + b44 * k4.v[c] + b45 * k5.v[c]);
-        x5[c] = si + dt * (b51 * k1.v[c] + b53 * k3.v[c] + b54 * k4.v[c] + b55 * k5.v[c] + b56 * k6.v[c]);
+        const double x4 = si + dt * (b41 * kk[0][c] + b43 * kk[2][c] + b44 * kk[3][c] + b45 * kk[4][c]);
+        x5[c] = si + dt * (b51 * kk[0][c] + b53 * kk[2][c] + b54 * kk[3][c] + b55 * kk[4][c] + b56 * k6.v[c]);
         const double sc = kp.atol + kp.rtol * fmax(fabs(x5[c]), fabs(x4));
         const double ratio = fabs(x5[c] - x4) / sc;
         if (!isfinite(x5[c]) || !isfinite(ratio)) finite = false;
