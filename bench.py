@@ -222,7 +222,9 @@ def run_ours(args):
     # form keeps the library's default shape
     cfg = None
     if "mixed_batched" in forms and not args.no_autotune:
-        cfg, _, _ = autotune.tune(forms["mixed_batched"], prepare, w.name, log=None)
+        cfg, _, table = autotune.tune(forms["mixed_batched"], prepare, w.name, log=None)
+        for c, ms in sorted(table, key=lambda x: x[1])[:8]:
+            log(f"autotune {c} {ms:.3f} ms")
     peak64, peak32 = lib.measure_fma_peaks()
 
     def one_step(ctx):

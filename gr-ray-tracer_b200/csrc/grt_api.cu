@@ -114,7 +114,7 @@ struct grt_ctx {
     DevBuf<unsigned long long> arrived;
     DevBuf<unsigned long long> scratch_u64;
     unsigned long long* host_u64 = nullptr;  // pinned
-    grt_launch_config lc{256, 1, 8, 32};
+    grt_launch_config lc{128, 4, 1, 32};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -279,7 +279,6 @@ grt_status grt_create(const grt_params* p, grt_ctx** out) {
         return GRT_ECUDA;
     }
     c->stream = c->own_stream;
-    c->lc.blocks_per_sm = 1;
     *out = c;
     return GRT_OK;
 }
@@ -329,10 +328,10 @@ grt_status grt_get_launch_config(const grt_ctx* c, grt_launch_config* cfg) {
 
 grt_status grt_set_launch_config(grt_ctx* c, const grt_launch_config* cfg) {
     if (!c || !cfg) return GRT_EINVAL;
-    if (cfg->threads_per_block < 32 || cfg->threads_per_block > 256 || cfg->threads_per_block % 32 != 0)
-        return fail(c, GRT_EINVAL, "threads_per_block must be a multiple of 32 in [32, 256]");
-    if (cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 32)
-        return fail(c, GRT_EINVAL, "blocks_per_sm must be in [1, 32]");
+    if (cfg->threads_per_block != 128)
+        return fail(c, GRT_EINVAL, "threads_per_block must be 128 (the trace kernels' block size)");
+    if (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 4)
+        return fail(c, GRT_EINVAL, "blocks_per_sm must be 2, 3 or 4 (register caps 255, 170, 128)");
     if (cfg->refill_threshold < 1 || cfg->refill_threshold > 32)
         return fail(c, GRT_EINVAL, "refill_threshold must be in [1, 32]");
     if (cfg->photons_per_grab < 1 || cfg->photons_per_grab > (1 << 20))
@@ -545,7 +544,7 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
     }
     grt::KParams kp = make_kparams(c);
     const size_t smem = c->separable ? (c->nr + c->nth + c->nph) * sizeof(double) : 0;
-    const int threads = c->lc.threads_per_block;
+    const int threads = 128;
     const int blocks = c->sm_count * c->lc.blocks_per_sm;
     const unsigned long long total = c->n;
     unsigned long long terminated = c->initial_terminated;
@@ -579,8 +578,8 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
         GRT_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, sizeof(grt::KCounters), c->stream), "memset counters");
         GRT_CUDA(c, cudaEventRecord(c->ev0, c->stream), "event");
         cudaError_t e = p.precision == GRT_PREC_MIXED
-                            ? grt::launch_trace_mixed(kp, p.integrator, blocks, threads, smem, c->stream)
-                            : grt::launch_trace_fp64(kp, p.integrator, blocks, threads, smem, c->stream);
+                            ? grt::launch_trace_mixed(kp, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream)
+                            : grt::launch_trace_fp64(kp, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
         if (e != cudaSuccess) return cuda_fail(c, e, "trace launch");
         GRT_CUDA(c, cudaEventRecord(c->ev1, c->stream), "event");
         GRT_CUDA(c, cudaMemcpyAsync(c->host_counters, c->counters.ptr, sizeof(grt::KCounters), cudaMemcpyDeviceToHost,

@@ -10,8 +10,10 @@
 
 namespace grt {
 
-template <int INTEGRATOR>
-__global__ void __launch_bounds__(256) trace_fp64(const __grid_constant__ KParams kp) {
+// 128-thread blocks; MINB resident blocks per SM caps the registers per
+// thread at 65536 / (128 * MINB): 255, 170 and 128 for MINB = 2, 3, 4.
+template <int INTEGRATOR, int MINB>
+__global__ void __launch_bounds__(128, MINB) trace_fp64(const __grid_constant__ KParams kp) {
     extern __shared__ double smem[];
     const double *s_r, *s_th, *s_ph;
     dev::stage_axes(kp, smem, s_r, s_th, s_ph);
@@ -101,16 +103,32 @@ __global__ void count_terminated(const uint8_t* __restrict__ term, unsigned long
 }
 
 // ---- host-side launchers ----
-cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int blocks, int threads, size_t smem,
-                              cudaStream_t stream) {
-    if (integrator == 0) {
-        cudaFuncSetAttribute(trace_fp64<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        trace_fp64<0><<<blocks, threads, smem, stream>>>(kp);
-    } else {
-        cudaFuncSetAttribute(trace_fp64<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        trace_fp64<1><<<blocks, threads, smem, stream>>>(kp);
-    }
+template <int I, int B>
+static cudaError_t launch_trace_fp64_v(const KParams& kp, int blocks, size_t smem, cudaStream_t stream) {
+    cudaFuncSetAttribute(trace_fp64<I, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    trace_fp64<I, B><<<blocks, 128, smem, stream>>>(kp);
     return cudaGetLastError();
+}
+
+// 128-thread blocks, sm_count * blocks_per_sm of them; blocks_per_sm (2, 3
+// or 4) selects the register-capped instantiation.
+cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int sm_count, int blocks_per_sm, size_t smem,
+                           cudaStream_t stream) {
+    const int blocks = sm_count * blocks_per_sm;
+    if (integrator == 0) {
+        switch (blocks_per_sm) {
+            case 2: return launch_trace_fp64_v<0, 2>(kp, blocks, smem, stream);
+            case 3: return launch_trace_fp64_v<0, 3>(kp, blocks, smem, stream);
+            case 4: return launch_trace_fp64_v<0, 4>(kp, blocks, smem, stream);
+            default: return cudaErrorInvalidConfiguration;
+        }
+    }
+    switch (blocks_per_sm) {
+        case 2: return launch_trace_fp64_v<1, 2>(kp, blocks, smem, stream);
+        case 3: return launch_trace_fp64_v<1, 3>(kp, blocks, smem, stream);
+        case 4: return launch_trace_fp64_v<1, 4>(kp, blocks, smem, stream);
+        default: return cudaErrorInvalidConfiguration;
+    }
 }
 
 cudaError_t launch_init_image(const InitImageArgs& args, cudaStream_t stream) {

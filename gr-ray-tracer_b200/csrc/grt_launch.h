@@ -32,9 +32,11 @@ struct ProductsArgs {
     unsigned long long* arrived;   // [1]
 };
 
-cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int blocks, int threads, size_t smem,
+// Persistent trace launches: sm_count * blocks_per_sm blocks of 128 threads;
+// blocks_per_sm in {2, 3, 4} picks the register cap (255 / 170 / 128).
+cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int sm_count, int blocks_per_sm, size_t smem,
                               cudaStream_t stream);
-cudaError_t launch_trace_mixed(const KParams& kp, int integrator, int blocks, int threads, size_t smem,
+cudaError_t launch_trace_mixed(const KParams& kp, int integrator, int sm_count, int blocks_per_sm, size_t smem,
                                cudaStream_t stream);
 cudaError_t launch_init_image(const InitImageArgs& args, cudaStream_t stream);
 cudaError_t launch_image_products(const ProductsArgs& args, cudaStream_t stream);

@@ -1,8 +1,9 @@
 """Launch-shape autotuner for the persistent trace kernel.
 
-Searches threads per block, resident blocks per SM, the per-warp refill
-threshold (idle lanes before a warp pulls new photons) and the photons a warp
-claims per queue access, timing each candidate with the library's own CUDA
+Searches the occupancy class (resident 128-thread blocks per SM, i.e. the
+register cap of the kernel instantiation), the per-warp refill threshold (idle
+lanes before a warp pulls new photons) and the photons a warp claims per queue
+access, timing each candidate with the library's own CUDA
 events around the trace launch on the actual workload.  Results are cached per
 (workload key, precision, integrator) for the life of the process.
 """
@@ -13,20 +14,19 @@ import itertools
 
 _CACHE: dict = {}
 
-THREADS = (64, 128, 256)
-REFILL = (1, 4, 8, 16, 32)
-GRAB = (32, 64, 256)
+BLOCKS_PER_SM = (2, 3, 4)   # 128-thread blocks; register caps 255 / 170 / 128
+REFILL = (1, 8, 16, 32)
+GRAB = (32, 128)
 
 
-def candidates(occupancy_threads: int = 256):
-    """Launch shapes with the same resident threads per SM (the kernel's
-    register footprint fixes occupancy), crossed with the queue knobs."""
-    for tpb, refill, grab in itertools.product(THREADS, REFILL, GRAB):
-        yield dict(threads_per_block=tpb, blocks_per_sm=max(1, occupancy_threads // tpb),
-                   refill_threshold=refill, photons_per_grab=grab)
+def candidates():
+    """Occupancy classes (resident 128-thread blocks per SM, which fix the
+    register cap of the instantiation) crossed with the queue knobs."""
+    for bps, refill, grab in itertools.product(BLOCKS_PER_SM, REFILL, GRAB):
+        yield dict(threads_per_block=128, blocks_per_sm=bps, refill_threshold=refill, photons_per_grab=grab)
 
 
-def tune(ctx, prepare, key, reps: int = 2, occupancy_threads: int = 256, log=None):
+def tune(ctx, prepare, key, reps: int = 2, log=None):
     """Pick the fastest launch shape for `ctx`.
 
     prepare(ctx) must reset the photons (e.g. re-initialise the pixel grid);
@@ -40,7 +40,7 @@ def tune(ctx, prepare, key, reps: int = 2, occupancy_threads: int = 256, log=Non
         return cfg, ms, table
     table = []
     best = None
-    for cfg in candidates(occupancy_threads):
+    for cfg in candidates():
         ctx.set_launch_config(**cfg)
         prepare(ctx)
         ctx.run()

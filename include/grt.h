@@ -156,10 +156,10 @@ typedef struct grt_image_products {
 
 /* Launch shape of the trace kernel (chosen by grt_autotune or set by hand). */
 typedef struct grt_launch_config {
-    int32_t threads_per_block;    /* multiple of 32, <= 1024 */
-    int32_t blocks_per_sm;        /* resident blocks launched per SM */
+    int32_t threads_per_block;    /* 128 (the trace kernels' block size) */
+    int32_t blocks_per_sm;        /* 2, 3 or 4 resident blocks per SM: register caps 255 / 170 / 128 */
     int32_t refill_threshold;     /* idle lanes in a warp before it pulls new photons (1..32) */
-    int32_t photons_per_grab;     /* photons a warp claims per queue access, multiple of 32 is not required */
+    int32_t photons_per_grab;     /* photons a warp claims per access to the global queue */
 } grt_launch_config;
 
 typedef struct grt_ctx grt_ctx;

@@ -37,9 +37,9 @@ def test_image_parity_fp64(gpu, oracle, w):
 
 
 @pytest.mark.parametrize("launch", [
-    dict(threads_per_block=64, blocks_per_sm=2, refill_threshold=1, photons_per_grab=32),
-    dict(threads_per_block=128, blocks_per_sm=1, refill_threshold=16, photons_per_grab=64),
-    dict(threads_per_block=256, blocks_per_sm=1, refill_threshold=32, photons_per_grab=4096),
+    dict(threads_per_block=128, blocks_per_sm=2, refill_threshold=1, photons_per_grab=32),
+    dict(threads_per_block=128, blocks_per_sm=3, refill_threshold=16, photons_per_grab=64),
+    dict(threads_per_block=128, blocks_per_sm=4, refill_threshold=32, photons_per_grab=4096),
 ])
 def test_launch_shapes_identical(gpu, oracle, launch):
     w = C2_MINI
