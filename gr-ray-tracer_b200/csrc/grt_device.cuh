@@ -286,6 +286,28 @@ GRT_DEV bool build_tetrad(const double g[4][4], const double u[4], double e[4][4
 // Cartesian velocity / magnetic four-vectors per cell are precomputed on the
 // host with the reference's transform (fluid_frame.hpp:28-48) and unit scale,
 // so the per-step arithmetic is exactly the reference's.
+// fluid_frame.hpp:28-48 on the device, times the [units] scale (raw layout only).
+GRT_DEV void spherical_to_cartesian_scaled(double r, double th, double ph, double spin, const double* sv,
+                                          double scale, double c[4]) {
+    double st, ct, sp, cp;
+    sincos(th, &st, &ct);
+    sincos(ph, &sp, &cp);
+    const double radial_x = cp * st, radial_y = sp * st, radial_z = ct;
+    const double theta_x = (r * cp - spin * sp) * ct;
+    const double theta_y = (r * sp + spin * cp) * ct;
+    const double theta_z = -r * st;
+    const double phi_x = (-r * sp - spin * cp) * st;
+    const double phi_y = (r * cp - spin * sp) * st;
+    c[0] = sv[0] * scale;
+    c[1] = (radial_x * sv[1] + theta_x * sv[2] + phi_x * sv[3]) * scale;
+    c[2] = (radial_y * sv[1] + theta_y * sv[2] + phi_y * sv[3]) * scale;
+    c[3] = (radial_z * sv[1] + theta_z * sv[2]) * scale;
+}
+
+// RAW selects the grid layout: false -- packed (rho, T) pairs and Cartesian
+// four-vectors precomputed on the host; true -- the reference's raw arrays,
+// with the spherical-to-Cartesian conversion done per sample.
+template <bool RAW = false>
 GRT_DEV bool sample_fluid(const KParams& kp, const double* s_r, const double* s_th, const double* s_ph,
                           const double s[8], double radius, FluidSample& out) {
     const KGrid& G = kp.grid;
@@ -317,21 +339,33 @@ GRT_DEV bool sample_fluid(const KParams& kp, const double* s_r, const double* s_
     f.position_cm[1] = s[2] * kp.length_scale;
     f.position_cm[2] = s[3] * kp.length_scale;
     f.coordinate_time_s = s[0] * kp.time_scale;
-    const double2 rt = G.rho_t[cell];
-    f.density_g_cm3 = rt.x * kp.density_scale;
-    f.temperature_k = rt.y * kp.temperature_scale;
-    if (!(f.density_g_cm3 > 0.0) || !isfinite(f.density_g_cm3) || !isfinite(f.temperature_k))
-        return false;
-    const double2 u01 = G.vel[2 * cell], u23 = G.vel[2 * cell + 1];
-    f.coordinate_four_velocity_cm_s[0] = u01.x;
-    f.coordinate_four_velocity_cm_s[1] = u01.y;
-    f.coordinate_four_velocity_cm_s[2] = u23.x;
-    f.coordinate_four_velocity_cm_s[3] = u23.y;
+    double cm[4];
+    if (RAW) {
+        f.density_g_cm3 = G.rho_raw[cell] * kp.density_scale;
+        f.temperature_k = G.T_raw[cell] * kp.temperature_scale;
+        if (!(f.density_g_cm3 > 0.0) || !isfinite(f.density_g_cm3) || !isfinite(f.temperature_k))
+            return false;
+        spherical_to_cartesian_scaled(G.r3[cell], G.th3[cell], G.ph3[cell], kp.a, G.vel_raw + 4 * cell,
+                                      G.vel_scale, f.coordinate_four_velocity_cm_s);
+        spherical_to_cartesian_scaled(G.r3[cell], G.th3[cell], G.ph3[cell], kp.a, G.mag_raw + 4 * cell,
+                                      G.mag_scale, cm);
+    } else {
+        const double2 rt = G.rho_t[cell];
+        f.density_g_cm3 = rt.x * kp.density_scale;
+        f.temperature_k = rt.y * kp.temperature_scale;
+        if (!(f.density_g_cm3 > 0.0) || !isfinite(f.density_g_cm3) || !isfinite(f.temperature_k))
+            return false;
+        const double2 u01 = G.vel[2 * cell], u23 = G.vel[2 * cell + 1];
+        f.coordinate_four_velocity_cm_s[0] = u01.x;
+        f.coordinate_four_velocity_cm_s[1] = u01.y;
+        f.coordinate_four_velocity_cm_s[2] = u23.x;
+        f.coordinate_four_velocity_cm_s[3] = u23.y;
+        const double2 b01 = G.mag[2 * cell], b23 = G.mag[2 * cell + 1];
+        cm[0] = b01.x; cm[1] = b01.y; cm[2] = b23.x; cm[3] = b23.y;
+    }
     MetricAt m;
     ks_metric_from_r(s[1], s[2], s[3], radius, kp.a, kp.M, m);
     if (!build_tetrad(m.g, f.coordinate_four_velocity_cm_s, out.e)) return false;
-    const double2 b01 = G.mag[2 * cell], b23 = G.mag[2 * cell + 1];
-    const double cm[4] = {b01.x, b01.y, b23.x, b23.y};
     f.magnetic_gauss[0] = -metric_dot(m.g, out.e[0], cm);
 #pragma unroll
     for (int axis = 1; axis < 4; ++axis) f.magnetic_gauss[axis] = metric_dot(m.g, out.e[axis], cm);

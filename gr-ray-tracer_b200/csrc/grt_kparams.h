@@ -25,6 +25,13 @@ struct KGrid {
     const double2* mag;     // [2*ncells] Cartesian KS b^mu * magnetic scale
     double r_reject_lo;     // radii outside [lo, hi] cannot pass within_radial_cell
     double r_reject_hi;
+    // Raw reference layout (allocation-free entry point): the seven arrays as
+    // loaded from the NumPy inputs, four-vectors converted per sample.
+    const double* rho_raw;  // [ncells]
+    const double* T_raw;    // [ncells]
+    const double* vel_raw;  // [ncells*4] spherical KS components
+    const double* mag_raw;  // [ncells*4]
+    double vel_scale, mag_scale;
 };
 
 // Device structure-of-arrays photon state (struct Photons, src/utils.hpp:40-133).

@@ -226,6 +226,7 @@ struct LaneCounters {
 // Everything after the integration step of one call (integrate_cart_ks.hpp:307-417).
 // phase0 is the phase loaded at the start of the call.  Returns 1 if the photon
 // terminated.
+template <bool RAW = false>
 GRT_DEV int post_step(const KParams& kp, const double* s_r, const double* s_th, const double* s_ph,
                       Lane& L, int phase0, double taken, int64_t step, double& tdisp, double& pdisp,
                       int& have_disp) {
@@ -234,7 +235,7 @@ GRT_DEV int post_step(const KParams& kp, const double* s_r, const double* s_th, 
     const bool backward = phase0 == 1;  // ImageBackward
     const bool needs = kp.scat_on || kp.abs_on || kp.emis_on || (kp.image_mode && backward);
     FluidSample fs;
-    const bool sampled = needs && sample_fluid(kp, s_r, s_th, s_ph, L.s, L.radius, fs);
+    const bool sampled = needs && sample_fluid<RAW>(kp, s_r, s_th, s_ph, L.s, L.radius, fs);
     int terminated = 0;
     if (kp.image_mode && backward && sampled) {
         Philox rng(kp.seed, L.id, static_cast<uint32_t>(step));
@@ -307,7 +308,7 @@ GRT_DEV int post_step(const KParams& kp, const double* s_r, const double* s_th, 
     return terminated;
 }
 
-template <int INTEGRATOR, class RHS>
+template <int INTEGRATOR, class RHS, bool RAW = false>
 GRT_DEV void trace_body(const KParams& kp, const double* s_r, const double* s_th, const double* s_ph) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -395,7 +396,7 @@ GRT_DEV void trace_body(const KParams& kp, const double* s_r, const double* s_th
                     rk4_step<RHS>(L.s, taken, kp, 1);
                     RHS::after_accept(L.s, kp, 1);
                     ++cnt.accepted;
-                    terminated = post_step(kp, s_r, s_th, s_ph, L, phase0, taken,
+                    terminated = post_step<RAW>(kp, s_r, s_th, s_ph, L, phase0, taken,
                                            kp.step0 + L.calls - 1, tdisp, pdisp, have_disp);
                     finished = terminated;
                 } else {
@@ -421,7 +422,7 @@ GRT_DEV void trace_body(const KParams& kp, const double* s_r, const double* s_th
                 L.dl = L.dl_try;
                 L.mid_call = 0;
                 const int phase0 = L.phase;
-                terminated = post_step(kp, s_r, s_th, s_ph, L, phase0, taken,
+                terminated = post_step<RAW>(kp, s_r, s_th, s_ph, L, phase0, taken,
                                        kp.step0 + L.calls - 1, tdisp, pdisp, have_disp);
                 finished = terminated;
             } else {

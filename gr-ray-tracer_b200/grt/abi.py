@@ -77,6 +77,12 @@ class PhotonSoA(C.Structure):
         ("terminate", _U8P), ("phase", _U8P)]
 
 
+class DeviceGrid(C.Structure):
+    """grt_device_grid: the seven grid arrays as device pointers (reference layout)."""
+    _fields_ = [("nr", _U64), ("ntheta", _U64), ("nphi", _U64)] + [
+        (n, C.c_void_p) for n in ("r", "theta", "phi", "rho", "temperature", "vel4", "mag4")]
+
+
 class RunStats(C.Structure):
     _fields_ = [("steps_done", _I64), ("n_terminated", _U64), ("accepted_steps", _U64),
                 ("rejected_attempts", _U64), ("photon_calls", _U64), ("launches", _U64),

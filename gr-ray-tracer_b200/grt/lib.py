@@ -14,8 +14,8 @@ from pathlib import Path
 
 import numpy as np
 
-from .abi import (GRT_OK, STATUS_NAMES, ImageProducts, LaunchConfig, Params, PhotonArrays, PhotonSoA,
-                  ProductArrays, RunStats)
+from .abi import (GRT_OK, STATUS_NAMES, DeviceGrid, ImageProducts, LaunchConfig, Params, PhotonArrays,
+                  PhotonSoA, ProductArrays, RunStats)
 
 PKG_ROOT = Path(__file__).resolve().parent.parent
 LIB_PATH = PKG_ROOT / "lib" / "libgrt_b200.so"
@@ -75,7 +75,9 @@ def load(path: Path | None = None):
     L.grt_get_launch_config.argtypes = [vp, P(LaunchConfig)]
     L.grt_set_launch_config.argtypes = [vp, P(LaunchConfig)]
     L.grt_measure_fma_peaks.argtypes = [P(C.c_double), P(C.c_double)]
-    for name in ("grt_measure_fma_peaks", "grt_params_validate", "grt_params_from_toml", "grt_create", "grt_set_params",
+    L.grt_trace_device_noalloc.argtypes = [P(Params), P(DeviceGrid), P(PhotonSoA), C.c_uint64, P(RunStats),
+                                           vp, C.c_char_p, C.c_size_t]
+    for name in ("grt_trace_device_noalloc", "grt_measure_fma_peaks", "grt_params_validate", "grt_params_from_toml", "grt_create", "grt_set_params",
                  "grt_set_stream", "grt_synchronize", "grt_upload_grid", "grt_upload_grid_numpy_dir",
                  "grt_upload_photons", "grt_init_image_photons", "grt_run", "grt_download_photons",
                  "grt_get_image_products", "grt_write_image_products_npz", "grt_get_launch_config",
@@ -117,6 +119,19 @@ def measure_fma_peaks():
     if rc != GRT_OK:
         raise GrtError(rc, "grt_measure_fma_peaks failed")
     return d.value, f.value
+
+
+def trace_device_noalloc(params: Params, grid: DeviceGrid, photons: PhotonSoA, n: int, stream_ptr=None):
+    """Allocation-free trace of n photons held in caller-owned device memory
+    (photons: PhotonSoA of device pointers; grid: DeviceGrid of device
+    pointers).  Returns the run statistics."""
+    st = RunStats()
+    err = C.create_string_buffer(512)
+    rc = load().grt_trace_device_noalloc(C.byref(params), C.byref(grid) if grid is not None else None,
+                                          C.byref(photons), n, C.byref(st), C.c_void_p(stream_ptr or 0), err, 512)
+    if rc != GRT_OK:
+        raise GrtError(rc, err.value.decode())
+    return st.as_dict()
 
 
 def _dp(a):

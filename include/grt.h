@@ -252,6 +252,46 @@ grt_status grt_get_launch_config(const grt_ctx* ctx, grt_launch_config* cfg);
 grt_status grt_set_launch_config(grt_ctx* ctx, const grt_launch_config* cfg);
 
 /*
+ * Fluid grid already in caller-owned device memory, in the reference's own
+ * layout: the seven NumPy inputs as C-order float64 arrays of shape
+ * (nr, ntheta, nphi) for r/theta/phi/rho/temperature and (nr, ntheta, nphi, 4)
+ * for vel4/mag4.  nr*ntheta*nphi == 0 means no fluid.
+ */
+typedef struct grt_device_grid {
+    uint64_t nr, ntheta, nphi;
+    const double* r;
+    const double* theta;
+    const double* phi;
+    const double* rho;
+    const double* temperature;
+    const double* vel4;
+    const double* mag4;
+} grt_device_grid;
+
+/*
+ * Allocation-free tracing (no counterpart in the reference).  For callers
+ * that cannot call cudaMalloc where they trace -- hosts whose device memory is
+ * owned by their own pool or a fixed budget, or latency-critical loops that
+ * must not allocate (cudaMalloc can synchronise the device) -- this traces
+ * n photons that already live in caller-owned device memory (`photons` holds
+ * DEVICE pointers here) against a grid in caller-owned device memory, in
+ * place, with the same step-loop semantics as grt_run and the FP64 parity
+ * kernel, on `stream` (a cudaStream_t, NULL = legacy default stream).
+ * It creates no context, allocates nothing and frees nothing.  Its scratch
+ * (work-queue head, counters, staged grid axes) is a 64 KiB array in the
+ * library that each GPU loading the library holds until exit, shared by all
+ * calls: serialise calls per device, because calls that overlap on the GPU
+ * race on it.  Limits: nr + ntheta + nphi <= 8160 (larger grids are rejected
+ * with GRT_EINVAL and a message), FP64 precision only.  The first call on a
+ * device looks up the scratch address (cudaGetSymbolAddress) with that device
+ * current; make it before any stream capture.  err receives a message on
+ * failure (may be NULL).
+ */
+grt_status grt_trace_device_noalloc(const grt_params* p, const grt_device_grid* grid,
+                                    const grt_photon_soa* photons, uint64_t n, grt_run_stats* stats,
+                                    void* stream, char* err, size_t err_len);
+
+/*
  * Roofline denominators (no counterpart in the reference): FP64 and FP32 FMA
  * throughput of the current device in TFLOP/s (2 flops per FMA), measured
  * with CUDA events over long independent FMA chains.
