@@ -7,7 +7,7 @@ import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
 PKG = ROOT / "gr-ray-tracer_b200"
-for p in (str(PKG), str(ROOT / "oracle"), str(ROOT / "tests")):
+for p in (str(PKG), str(ROOT / "oracle"), str(ROOT / "tests"), str(ROOT / "tests" / "golden")):
     if p not in sys.path:
         sys.path.insert(0, p)
 

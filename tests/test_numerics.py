@@ -1,0 +1,46 @@
+"""Pinned numerics of the oracle: the algorithmic op counts the roofline uses
+and the correctly rounded fourth root of the RK45 controller."""
+
+import ctypes as C
+import math
+import random
+
+import numpy as np
+import pytest
+
+from grt import workloads
+
+_DP = C.POINTER(C.c_double)
+
+
+def test_op_counts_pinned(oracle):
+    # One RHS = 243 ops, one RK4 step = 1100, one RKF45 attempt (k1 given) =
+    # 1691, counted over the reference's source operations (add/sub, mul, div,
+    # sqrt, pow each 1) by a counting scalar type that reproduces the double
+    # results exactly (checks == 0).
+    import bench
+    p = workloads.C2.params()
+    ok, P = oracle.null_momentum([0.0, 6.0, 2.0, 1.0], [-0.4, 0.8, 0.2], p.spin, p.mass)
+    X = np.array([0.0, 6.0, 2.0, 1.0])
+    a = (C.c_uint64 * 5)(); b = (C.c_uint64 * 5)(); c = (C.c_uint64 * 5)(); ch = (C.c_double * 3)()
+    oracle.lib.oracle_op_counts(C.byref(p), X.ctypes.data_as(_DP), P.ctypes.data_as(_DP), C.c_double(0.3),
+                                a, b, c, ch)
+    assert list(ch) == [0.0, 0.0, 0.0]
+    assert sum(a) == bench.OPS_RHS == 243
+    assert sum(b) == bench.OPS_RK4_STEP == 1100
+    assert sum(c) == bench.OPS_RK45_ATTEMPT == 1691
+    assert list(a) == [61, 159, 21, 2, 0]
+
+
+def test_fourth_root_correctly_rounded(oracle):
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.prec = 300
+    random.seed(11)
+    xs = [10 ** random.uniform(-300, 300) for _ in range(4000)]
+    xs += [10 ** random.uniform(-12, 8) for _ in range(4000)]
+    xs += [5e-324, 1e-310, 2.0 ** -1022, 1.0, 16.0, 0.5, 2.0, 1.7976931348623157e308]
+    for x in xs:
+        want = float(mpmath.mpf(x) ** mpmath.mpf(0.25))
+        assert oracle.lib.oracle_fourth_root(x) == want, x
+    assert oracle.lib.oracle_fourth_root(0.0) == 0.0
+    assert math.isinf(oracle.lib.oracle_fourth_root(math.inf))
