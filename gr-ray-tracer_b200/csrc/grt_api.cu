@@ -101,7 +101,7 @@ struct grt_ctx {
     bool separable = false;
     int nr = 0, nth = 0, nph = 0;
     double r_reject_lo = 0.0, r_reject_hi = 0.0;
-    DevBuf<double> r_axis, th_axis, ph_axis, r3, th3, ph3;
+    DevBuf<double> r_axis, th_axis, ph_axis, r_half, th_half, ph_half, r3, th3, ph3;
     DevBuf<double2> rho_t, vel, mag;
     // photons
     size_t n = 0;
@@ -154,6 +154,36 @@ void spherical_to_cartesian_vec(double r, double th, double ph, double spin, con
     c[2] = radial_y * s[1] + theta_y * s[2] + phi_y * s[3];
     c[3] = radial_z * s[1] + theta_z * s[2];
     for (int q = 0; q < 4; ++q) c[q] *= scale;
+}
+
+// scattering.hpp:99-149: the acceptance half-width 0.500001 * (largest
+// neighbour span) of each separable axis value, evaluated with glibc like the
+// reference evaluates it on every call.
+double periodic_distance(double lhs, double rhs) {
+    const double d = std::fmod(std::fabs(lhs - rhs), 2.0 * kPi);
+    return std::fmin(d, 2.0 * kPi - d);
+}
+std::vector<double> half_spans(const std::vector<double>& a, int kind) {
+    const size_t n = a.size();
+    std::vector<double> h(n);
+    for (size_t i = 0; i < n; ++i) {
+        if (n == 1) {
+            h[i] = 1.0e-10;
+            continue;
+        }
+        double span = 0.0;
+        for (int side = 0; side < 2; ++side) {
+            if ((side == 0 && i == 0) || (side == 1 && i + 1 >= n)) continue;
+            const double nb = a[side == 0 ? i - 1 : i + 1];
+            double d;
+            if (kind == 0) d = std::fabs(std::log(a[i] / nb));
+            else if (kind == 1) d = std::fabs(a[i] - nb);
+            else d = periodic_distance(a[i], nb);
+            span = std::fmax(span, d);
+        }
+        h[i] = 0.500001 * span;
+    }
+    return h;
 }
 
 bool well_separated_increasing(const std::vector<double>& a) {
@@ -222,6 +252,9 @@ grt::KParams make_kparams(const grt_ctx* c) {
     g.r_axis = c->r_axis.ptr;
     g.th_axis = c->th_axis.ptr;
     g.ph_axis = c->ph_axis.ptr;
+    g.r_half = c->r_half.ptr;
+    g.th_half = c->th_half.ptr;
+    g.ph_half = c->ph_half.ptr;
     g.r3 = c->r3.ptr;
     g.th3 = c->th3.ptr;
     g.ph3 = c->ph3.ptr;
@@ -287,6 +320,7 @@ void grt_destroy(grt_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->r_axis.release(); c->th_axis.release(); c->ph_axis.release();
+    c->r_half.release(); c->th_half.release(); c->ph_half.release();
     c->r3.release(); c->th3.release(); c->ph3.release();
     c->rho_t.release(); c->vel.release(); c->mag.release();
     c->ph.release();
@@ -405,6 +439,15 @@ grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const 
     GRT_CUDA(c, cudaMemcpy(c->r_axis.ptr, ra.data(), nr * sizeof(double), cudaMemcpyHostToDevice), "H2D axis");
     GRT_CUDA(c, cudaMemcpy(c->th_axis.ptr, ta.data(), nth * sizeof(double), cudaMemcpyHostToDevice), "H2D axis");
     GRT_CUDA(c, cudaMemcpy(c->ph_axis.ptr, pa.data(), nph * sizeof(double), cudaMemcpyHostToDevice), "H2D axis");
+    if (sep) {
+        const std::vector<double> rh = half_spans(ra, 0), th_h = half_spans(ta, 1), ph_h = half_spans(pa, 2);
+        GRT_CUDA(c, c->r_half.alloc(nr), "alloc half");
+        GRT_CUDA(c, c->th_half.alloc(nth), "alloc half");
+        GRT_CUDA(c, c->ph_half.alloc(nph), "alloc half");
+        GRT_CUDA(c, cudaMemcpy(c->r_half.ptr, rh.data(), nr * sizeof(double), cudaMemcpyHostToDevice), "H2D half");
+        GRT_CUDA(c, cudaMemcpy(c->th_half.ptr, th_h.data(), nth * sizeof(double), cudaMemcpyHostToDevice), "H2D half");
+        GRT_CUDA(c, cudaMemcpy(c->ph_half.ptr, ph_h.data(), nph * sizeof(double), cudaMemcpyHostToDevice), "H2D half");
+    }
     if (!sep) {
         GRT_CUDA(c, c->r3.alloc(ncell), "alloc r3");
         GRT_CUDA(c, c->th3.alloc(ncell), "alloc th3");
@@ -543,8 +586,9 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
         return GRT_OK;
     }
     grt::KParams kp = make_kparams(c);
-    const size_t smem = c->separable ? (c->nr + c->nth + c->nph) * sizeof(double) : 0;
     const int threads = 128;
+    const size_t smem = grt::dev_trace_smem_bytes(p.integrator, threads, c->fluid_available && c->separable, c->nr,
+                                                  c->nth, c->nph);
     const int blocks = c->sm_count * c->lc.blocks_per_sm;
     const unsigned long long total = c->n;
     unsigned long long terminated = c->initial_terminated;

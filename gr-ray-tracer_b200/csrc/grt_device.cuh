@@ -109,45 +109,37 @@ GRT_DEV int nearest_polar_sorted(const double* th, int n, double polar) {
     return dhi < dlo ? lo + 1 : lo;
 }
 
+// periodic_angle_distance for |lhs - rhs| <= 4 pi: fmod(v, 2 pi) is v, or
+// exactly v - 2 pi (Sterbenz) for v in [2 pi, 4 pi).  The separable path has
+// azimuth queries in [0, 2 pi] and axis values in [0, 2 pi).
+GRT_DEV double periodic_angle_distance_near(double lhs, double rhs) {
+    const double v = fabs(lhs - rhs);
+    const double d = v >= 2.0 * kPi ? v - 2.0 * kPi : v;
+    return fmin(d, 2.0 * kPi - d);
+}
+
 GRT_DEV int nearest_azimuth_sorted(const double* ph, int n, double az) {
     if (n == 1) return 0;
     const int lo = bracket(ph, n, az);
     const int c1 = lo < 0 ? n - 1 : lo;
     const int c2 = lo + 1 < n ? lo + 1 : 0;
-    const double d1 = periodic_angle_distance(az, ph[c1]);
-    const double d2 = periodic_angle_distance(az, ph[c2]);
+    const double d1 = periodic_angle_distance_near(az, ph[c1]);
+    const double d2 = periodic_angle_distance_near(az, ph[c2]);
     if (d1 < d2) return c1;
     if (d2 < d1) return c2;
     return c1 < c2 ? c1 : c2;
 }
 
-// scattering.hpp:99-149 on one separable axis.
-GRT_DEV bool within_radial_sorted(const double* r, int n, int i, double radius) {
-    const double center = r[i];
-    const double cd = fabs(log(radius / center));
-    if (n == 1) return cd <= 1.0e-10;
-    double span = 0.0;
-    if (i > 0) span = fmax(span, fabs(log(center / r[i - 1])));
-    if (i + 1 < n) span = fmax(span, fabs(log(center / r[i + 1])));
-    return cd <= 0.500001 * span;
+// scattering.hpp:99-149 on one separable axis, with the neighbour half-span
+// precomputed per axis value (see KGrid::r_half).
+GRT_DEV bool within_radial_sorted(const double* r, const double* half, int i, double radius) {
+    return fabs(log(radius / r[i])) <= half[i];
 }
-GRT_DEV bool within_polar_sorted(const double* th, int n, int j, double polar) {
-    const double center = th[j];
-    const double cd = fabs(polar - center);
-    if (n == 1) return cd <= 1.0e-10;
-    double span = 0.0;
-    if (j > 0) span = fmax(span, fabs(center - th[j - 1]));
-    if (j + 1 < n) span = fmax(span, fabs(center - th[j + 1]));
-    return cd <= 0.500001 * span;
+GRT_DEV bool within_polar_sorted(const double* th, const double* half, int j, double polar) {
+    return fabs(polar - th[j]) <= half[j];
 }
-GRT_DEV bool within_azimuth_sorted(const double* ph, int n, int k, double az) {
-    const double center = ph[k];
-    const double cd = periodic_angle_distance(az, center);
-    if (n == 1) return cd <= 1.0e-10;
-    double span = 0.0;
-    if (k > 0) span = fmax(span, periodic_angle_distance(center, ph[k - 1]));
-    if (k + 1 < n) span = fmax(span, periodic_angle_distance(center, ph[k + 1]));
-    return cd <= 0.500001 * span;
+GRT_DEV bool within_azimuth_sorted(const double* ph, const double* half, int k, double az) {
+    return periodic_angle_distance_near(az, ph[k]) <= half[k];
 }
 
 // General (non-separable) coordinates: the reference's three coordinate-descent
@@ -307,26 +299,35 @@ GRT_DEV void spherical_to_cartesian_scaled(double r, double th, double ph, doubl
 // RAW selects the grid layout: false -- packed (rho, T) pairs and Cartesian
 // four-vectors precomputed on the host; true -- the reference's raw arrays,
 // with the spherical-to-Cartesian conversion done per sample.
-template <bool RAW = false>
-GRT_DEV bool sample_fluid(const KParams& kp, const double* s_r, const double* s_th, const double* s_ph,
-                          const double s[8], double radius, FluidSample& out) {
+// Separable axes and their half-spans staged in shared memory.
+struct Axes {
+    const double* r;
+    const double* th;
+    const double* ph;
+    const double* rh;
+    const double* thh;
+    const double* phh;
+};
+
+template <bool RAW>
+static __device__ __noinline__ bool sample_fluid_at(const KParams& kp, const Axes ax, double t, double x,
+                                                    double y, double z, double radius, FluidSample* outp) {
+    FluidSample& out = *outp;
+    const double s[4] = {t, x, y, z};
     const KGrid& G = kp.grid;
-    if (!G.available) return false;
-    if (!(radius > 0.0) || !isfinite(radius)) return false;
-    if (radius < G.r_reject_lo || radius > G.r_reject_hi) return false;
     int i, j, k;
     if (G.separable) {
-        i = nearest_radial_sorted(s_r, G.nr, radius);
-        if (!within_radial_sorted(s_r, G.nr, i, radius)) return false;
+        i = nearest_radial_sorted(ax.r, G.nr, radius);
+        if (!within_radial_sorted(ax.r, ax.rh, i, radius)) return false;
     }
     const double ct = fmax(-1.0, fmin(1.0, s[3] / radius));
     const double polar = acos(ct);
     double az = atan2(radius * s[2] - kp.a * s[1], radius * s[1] + kp.a * s[2]);
     if (az < 0.0) az += 2.0 * kPi;
     if (G.separable) {
-        j = nearest_polar_sorted(s_th, G.nth, polar);
-        k = nearest_azimuth_sorted(s_ph, G.nph, az);
-        if (!within_polar_sorted(s_th, G.nth, j, polar) || !within_azimuth_sorted(s_ph, G.nph, k, az))
+        j = nearest_polar_sorted(ax.th, G.nth, polar);
+        k = nearest_azimuth_sorted(ax.ph, G.nph, az);
+        if (!within_polar_sorted(ax.th, ax.thh, j, polar) || !within_azimuth_sorted(ax.ph, ax.phh, k, az))
             return false;
     } else {
         const Grid3 g3{G.r3, G.th3, G.ph3, G.nr, G.nth, G.nph};
@@ -372,15 +373,37 @@ GRT_DEV bool sample_fluid(const KParams& kp, const double* s_r, const double* s_
     return true;
 }
 
+// sample_scattering_fluid (scattering.hpp:185-251): the cheap early-outs
+// inline, the lookup + gather + tetrad out of line.
+template <bool RAW = false>
+GRT_DEV bool sample_fluid(const KParams& kp, const Axes& ax, const double s[8], double radius, FluidSample& out) {
+    const KGrid& G = kp.grid;
+    if (!G.available) return false;
+    if (!(radius > 0.0) || !isfinite(radius)) return false;
+    if (radius < G.r_reject_lo || radius > G.r_reject_hi) return false;
+    return sample_fluid_at<RAW>(kp, ax, s[0], s[1], s[2], s[3], radius, &out);
+}
+
 // ---------------------------------------------------------------------------
 // Scattering and packet generation
 // ---------------------------------------------------------------------------
 constexpr double kProtonMassCgs = 1.67262192369e-24;   // scattering.hpp:256
 constexpr double kSigmaThomsonCgs = 6.6524587158e-25;  // scattering.hpp:257
 
-// maybe_scatter_photon (scattering.hpp:259-313)
-static __device__ __noinline__ bool maybe_scatter(double s[8], double I[4], double albedo, double dl, double length_scale,
+// State a scattering event may change, passed by copy to the out-of-line
+// maybe_scatter so the caller's state never has its address taken (which would
+// keep it in local memory for the whole trace loop).
+struct ScatterState {
+    double s[8];
+    double I[4];
+};
+
+// maybe_scatter_photon (scattering.hpp:259-313); st is changed only when it
+// returns true.
+static __device__ __noinline__ bool maybe_scatter(ScatterState* st, double albedo, double dl, double length_scale,
                            const FluidSample& fs, double a, double M, Philox& rng) {
+    double* s = st->s;
+    double* I = st->I;
     const double path_cm = dl * length_scale;
     const double ne = fs.fluid.density_g_cm3 / kProtonMassCgs;
     const double tau = kSigmaThomsonCgs * ne * path_cm;
@@ -467,12 +490,17 @@ GRT_DEV int camera_crossing(const KParams& kp, const double s[8], double& u, dou
     return inside ? 1 : -1;
 }
 
-GRT_DEV double camera_observer_energy(const KParams& kp, const double s[8]) {
+static __device__ __noinline__ double camera_observer_energy_at(double a, double M, double x, double y, double z,
+                                                                double pt) {
     MetricAt m;
-    ks_metric(s[1], s[2], s[3], kp.a, kp.M, m);
+    ks_metric(x, y, z, a, M, m);
     if (!(m.g[0][0] < 0.0)) return 0.0;
     const double u0 = 1.0 / sqrt(-m.g[0][0]);
-    return -s[4] * u0;
+    return -pt * u0;
+}
+
+GRT_DEV double camera_observer_energy(const KParams& kp, const double s[8]) {
+    return camera_observer_energy_at(kp.a, kp.M, s[1], s[2], s[3], s[4]);
 }
 
 }  // namespace dev

@@ -15,9 +15,10 @@ namespace grt {
 template <int INTEGRATOR, int MINB>
 __global__ void __launch_bounds__(128, MINB) trace_fp64(const __grid_constant__ KParams kp) {
     extern __shared__ double smem[];
-    const double *s_r, *s_th, *s_ph;
-    dev::stage_axes(kp, smem, s_r, s_th, s_ph);
-    dev::trace_body<INTEGRATOR, dev::Fp64Rhs>(kp, s_r, s_th, s_ph);
+    dev::Axes ax;
+    dev::KStore kk;
+    dev::stage_grid(kp, smem, INTEGRATOR, ax, kk);
+    dev::trace_body<INTEGRATOR, dev::Fp64Rhs>(kp, ax, kk);
 }
 
 // initialize_photons.hpp:116-169 with screen (u, v) at pixel centres; the

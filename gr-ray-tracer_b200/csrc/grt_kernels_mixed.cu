@@ -80,9 +80,10 @@ struct MixedRhs {
 template <int INTEGRATOR, int MINB>
 __global__ void __launch_bounds__(128, MINB) trace_mixed(const __grid_constant__ KParams kp) {
     extern __shared__ double smem[];
-    const double *s_r, *s_th, *s_ph;
-    dev::stage_axes(kp, smem, s_r, s_th, s_ph);
-    dev::trace_body<INTEGRATOR, dev::MixedRhs>(kp, s_r, s_th, s_ph);
+    dev::Axes ax;
+    dev::KStore kk;
+    dev::stage_grid(kp, smem, INTEGRATOR, ax, kk);
+    dev::trace_body<INTEGRATOR, dev::MixedRhs>(kp, ax, kk);
 }
 
 template <int I, int B>

@@ -17,6 +17,12 @@ struct KGrid {
     const double* r_axis;   // [nr]   separable axes (staged into shared memory)
     const double* th_axis;  // [nth]
     const double* ph_axis;  // [nph]
+    // within-cell acceptance half-widths per separable axis value, computed
+    // on the host exactly as scattering.hpp:99-149 computes them per call:
+    // 0.500001 * (largest neighbour span), or 1e-10 for a one-value axis
+    const double* r_half;   // [nr]   (log spacing)
+    const double* th_half;  // [nth]
+    const double* ph_half;  // [nph]  (periodic spacing)
     const double* r3;       // [nr*nth*nph] full coordinates (general path)
     const double* th3;
     const double* ph3;

@@ -32,6 +32,14 @@ struct ProductsArgs {
     unsigned long long* arrived;   // [1]
 };
 
+// Dynamic shared memory of a trace launch: k2..k5 slots for RK45 (4*7 doubles
+// per thread) plus the separable axes and their half-spans (2*(nr+nth+nph)).
+inline size_t dev_trace_smem_bytes(int integrator, int threads, bool separable, int nr, int nth, int nph) {
+    size_t n = integrator == 1 ? static_cast<size_t>(4 * 7) * threads : 0;
+    if (separable) n += 2 * static_cast<size_t>(nr + nth + nph);
+    return n * sizeof(double);
+}
+
 // Persistent trace launches: sm_count * blocks_per_sm blocks of 128 threads;
 // blocks_per_sm in {2, 3, 4} picks the register cap (255 / 170 / 128).
 cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int sm_count, int blocks_per_sm, size_t smem,

@@ -10,7 +10,7 @@
 // The only scratch the trace needs beyond its inputs and outputs -- the work
 // queue head and launch counters, plus the separable grid axes and lookup
 // bounds derived from the coordinate arrays -- lives in one file-scope
-// __device__ array of kNoallocScratchBytes (64 KiB) that every GPU which loads
+// __device__ array of kNoallocScratchBytes (128 KiB) that every GPU which loads
 // this library holds until the process exits.  All calls share it: each call
 // clears the parts that must start at zero, and calls that overlap on the GPU
 // (two streams, two host threads) race on it, so serialise calls per device.
@@ -25,15 +25,16 @@
 
 #include "grt.h"
 #include "grt_kparams.h"
+#include "grt_launch.h"
 #include "grt_trace.cuh"
 
 namespace {
 
-constexpr size_t kNoallocScratchBytes = 64 * 1024;
+constexpr size_t kNoallocScratchBytes = 128 * 1024;
 constexpr size_t kCountersOffset = 0;                      // grt::KCounters
 constexpr size_t kMetaOffset = 128;                        // GridMeta
-constexpr size_t kAxesOffset = 256;                        // r, theta, phi axes (doubles)
-constexpr size_t kMaxAxisValues = (kNoallocScratchBytes - kAxesOffset) / sizeof(double);
+constexpr size_t kAxesOffset = 256;                        // r, theta, phi axes, then their half-spans
+constexpr size_t kMaxAxisValues = 8160;                    // 2 * 8160 doubles fit after kAxesOffset
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
@@ -89,6 +90,28 @@ __global__ void noalloc_prepare_grid(const double* r, const double* th, const do
     for (int j = threadIdx.x; j < nth; j += blockDim.x) ta[j] = th[static_cast<long long>(j) * nph];
     for (int k = threadIdx.x; k < nph; k += blockDim.x) pa[k] = ph[k];
     __syncthreads();
+    // acceptance half-widths (scattering.hpp:99-149), as the host computes them
+    double* rh = pa + nph;
+    double* thh = rh + nr;
+    double* phh = thh + nth;
+    for (int q = threadIdx.x; q < nr + nth + nph; q += blockDim.x) {
+        const double* a;
+        double* h;
+        int n, i, kind;
+        if (q < nr) { a = ra; h = rh; n = nr; i = q; kind = 0; }
+        else if (q < nr + nth) { a = ta; h = thh; n = nth; i = q - nr; kind = 1; }
+        else { a = pa; h = phh; n = nph; i = q - nr - nth; kind = 2; }
+        double span = 0.0;
+        for (int side = 0; side < 2; ++side) {
+            if ((side == 0 && i == 0) || (side == 1 && i + 1 >= n)) continue;
+            const double nb = a[side == 0 ? i - 1 : i + 1];
+            const double d = kind == 0 ? fabs(log(a[i] / nb)) : kind == 1 ? fabs(a[i] - nb)
+                                                                          : grt::dev::periodic_angle_distance(a[i], nb);
+            span = fmax(span, d);
+        }
+        h[i] = n == 1 ? 1.0e-10 : 0.500001 * span;
+    }
+    __syncthreads();
     auto separated = [](const double* a, int n, int t) {
         for (int q = t + 1; q < n; q += blockDim.x) {
             if (!(a[q] > a[q - 1])) return false;
@@ -124,9 +147,10 @@ __global__ void noalloc_count_terminated(const uint8_t* term, unsigned long long
 template <int INTEGRATOR>
 __global__ void __launch_bounds__(128, 4) trace_noalloc(const __grid_constant__ grt::KParams kp) {
     extern __shared__ double smem[];
-    const double *s_r, *s_th, *s_ph;
-    grt::dev::stage_axes(kp, smem, s_r, s_th, s_ph);
-    grt::dev::trace_body<INTEGRATOR, grt::dev::Fp64Rhs, true>(kp, s_r, s_th, s_ph);
+    grt::dev::Axes ax;
+    grt::dev::KStore kk;
+    grt::dev::stage_grid(kp, smem, INTEGRATOR, ax, kk);
+    grt::dev::trace_body<INTEGRATOR, grt::dev::Fp64Rhs, true>(kp, ax, kk);
 }
 
 grt_status set_err(char* err, size_t len, const char* msg) {
@@ -227,6 +251,9 @@ extern "C" grt_status grt_trace_device_noalloc(const grt_params* p, const grt_de
     g.r_axis = axes;
     g.th_axis = axes + nr;
     g.ph_axis = axes + nr + nth;
+    g.r_half = axes + nr + nth + nph;
+    g.th_half = g.r_half + nr;
+    g.ph_half = g.th_half + nth;
     if (ncell) {
         g.r3 = grid->r;
         g.th3 = grid->theta;
@@ -271,7 +298,8 @@ extern "C" grt_status grt_trace_device_noalloc(const grt_params* p, const grt_de
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_fail(e);
     }
-    const size_t smem = gm.separable ? (nr + nth + nph) * sizeof(double) : 0;
+    const size_t smem = grt::dev_trace_smem_bytes(p->integrator, 128, gm.separable != 0, static_cast<int>(nr),
+                                                  static_cast<int>(nth), static_cast<int>(nph));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

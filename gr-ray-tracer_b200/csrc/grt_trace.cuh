@@ -73,6 +73,7 @@ struct Lane {
     int mid_call;
     int attempts;
     int fast;             // precision hint of the current call (mixed form)
+    int need_k1;          // the call's k1 = f(state) is still to be evaluated
     double dl_try;
     V7 k1;
 };
@@ -152,34 +153,65 @@ static __constant__ double kFehlbergA[5][5] = {
     {a51, a52, a53, a54, 0.0},
     {a61, a62, a63, a64, a65}};
 
-// One Fehlberg attempt (integrate_cart_ks.hpp:159-227); returns 1 if accepted
-// (s advanced), 0 if rejected; *dl receives the next proposed step either way.
-// The five stage evaluations share one right-hand-side site in a rolled loop
-// (k1..k5 live in thread-local memory); each stage input is summed over
-// j = 1..t-1 left to right, exactly the reference's association.  For the
-// first stage, dt*(a21 k1) equals the reference's (dt*a21)*k1 because
-// a21 = 1/4 is a power of two.
+// Trace kernels run kTraceThreads-thread blocks (the launchers and
+// __launch_bounds__ use the same constant).
+constexpr int kTraceThreads = 128;
+
+// Per-thread slots for k2..k5 in shared memory: [4][7][kTraceThreads] doubles,
+// thread-contiguous so a warp's accesses are conflict-free; base already
+// points at this thread's column, so a slot is a constant offset from it.
+struct KStore {
+    double* base;
+    GRT_DEV double& at(int j, int c) const { return base[(j * 7 + c) * kTraceThreads]; }
+};
+
+// pow(1/err, 0.25) of the reference, correctly rounded (grt_fourth_root.cuh);
+// out of line to keep the step loop small.
+static __device__ __noinline__ double controller_root(double x) { return fourth_root_cr(x); }
+
+// One Fehlberg attempt (integrate_cart_ks.hpp:159-227), preceded by the
+// call's k1 = f(state) when need_k1 (integrate_cart_ks.hpp:274-275); returns 1
+// if accepted (s advanced), 0 if rejected; *dl receives the next proposed step
+// either way.  All right-hand sides go through one site in a rolled stage
+// loop -- a lane that needs k1 runs it one iteration ahead of the others, so
+// the warp stays converged on the same code -- and k2..k5 live in shared
+// memory.  Each stage input is summed over j = 1..t-1 left to right, the
+// reference's association; for the first stage, dt*(a21 k1) equals the
+// reference's (dt*a21)*k1 because a21 = 1/4 is a power of two.
 template <class RHS>
-GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, const V7& k1, int fast) {
+GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, V7& k1, int need_k1, int fast,
+                         const KStore& kk) {
     const double dt = *dl;
-    double kk[5][7];
     V7 k6;
-#pragma unroll
-    for (int c = 0; c < 7; ++c) kk[0][c] = k1.v[c];
     double t[8];
     t[4] = s[4];
 #pragma unroll 1
-    for (int st = 0; st < 5; ++st) {
+    for (int st = need_k1 ? -1 : 0; st < 5; ++st) {
+        if (st < 0) {
 #pragma unroll
-        for (int c = 0; c < 7; ++c) {
-            double acc = kFehlbergA[st][0] * kk[0][c];
-            for (int j = 1; j <= st; ++j) acc = acc + kFehlbergA[st][j] * kk[j][c];
-            t[sidx(c)] = s[sidx(c)] + dt * acc;
+            for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)];
+        } else {
+            double acc[7];
+            const double a0 = kFehlbergA[st][0];
+#pragma unroll
+            for (int c = 0; c < 7; ++c) acc[c] = a0 * k1.v[c];
+#pragma unroll
+            for (int j = 1; j <= 4; ++j) {
+                if (j <= st) {
+                    const double aj = kFehlbergA[st][j];
+#pragma unroll
+                    for (int c = 0; c < 7; ++c) acc[c] = acc[c] + aj * kk.at(j - 1, c);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + dt * acc[c];
         }
         const V7 k = RHS::eval(t, kp, fast);
-        if (st < 4) {
+        if (st < 0) {
+            k1 = k;
+        } else if (st < 4) {
 #pragma unroll
-            for (int c = 0; c < 7; ++c) kk[st + 1][c] = k.v[c];
+            for (int c = 0; c < 7; ++c) kk.at(st, c) = k.v[c];
         } else {
             k6 = k;
         }
@@ -190,8 +222,9 @@ GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, const V7& k
 #pragma unroll
     for (int c = 0; c < 7; ++c) {
         const double si = s[sidx(c)];
-        const double x4 = si + dt * (b41 * kk[0][c] + b43 * kk[2][c] + b44 * kk[3][c] + b45 * kk[4][c]);
-        x5[c] = si + dt * (b51 * kk[0][c] + b53 * kk[2][c] + b54 * kk[3][c] + b55 * kk[4][c] + b56 * k6.v[c]);
+        const double k3 = kk.at(1, c), k4 = kk.at(2, c), k5 = kk.at(3, c);
+        const double x4 = si + dt * (b41 * k1.v[c] + b43 * k3 + b44 * k4 + b45 * k5);
+        x5[c] = si + dt * (b51 * k1.v[c] + b53 * k3 + b54 * k4 + b55 * k5 + b56 * k6.v[c]);
         const double sc = kp.atol + kp.rtol * fmax(fabs(x5[c]), fabs(x4));
         const double ratio = fabs(x5[c] - x4) / sc;
         if (!isfinite(x5[c]) || !isfinite(ratio)) finite = false;
@@ -207,8 +240,7 @@ GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, const V7& k
         for (int c = 0; c < 7; ++c) s[sidx(c)] = x5[c];
         return 1;
     }
-    // pow(1/err, 0.25) of the reference, correctly rounded (see grt_fourth_root.cuh)
-    double scale = kp.safety * fourth_root_cr(1.0 / err);
+    double scale = kp.safety * controller_root(1.0 / err);
     scale = fmin(kp.max_scale, fmax(kp.min_scale, scale));
     *dl = dt * scale;
     if (err <= 1.0) {
@@ -227,15 +259,14 @@ struct LaneCounters {
 // phase0 is the phase loaded at the start of the call.  Returns 1 if the photon
 // terminated.
 template <bool RAW = false>
-GRT_DEV int post_step(const KParams& kp, const double* s_r, const double* s_th, const double* s_ph,
-                      Lane& L, int phase0, double taken, int64_t step, double& tdisp, double& pdisp,
-                      int& have_disp) {
+GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, double taken, int64_t step,
+                      double& tdisp, double& pdisp, int& have_disp) {
     L.radius = ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
     L.have_radius = 1;
     const bool backward = phase0 == 1;  // ImageBackward
     const bool needs = kp.scat_on || kp.abs_on || kp.emis_on || (kp.image_mode && backward);
     FluidSample fs;
-    const bool sampled = needs && sample_fluid<RAW>(kp, s_r, s_th, s_ph, L.s, L.radius, fs);
+    const bool sampled = needs && sample_fluid<RAW>(kp, ax, L.s, L.radius, fs);
     int terminated = 0;
     if (kp.image_mode && backward && sampled) {
         Philox rng(kp.seed, L.id, static_cast<uint32_t>(step));
@@ -280,7 +311,17 @@ GRT_DEV int post_step(const KParams& kp, const double* s_r, const double* s_th, 
         }
         if (kp.scat_on) {
             Philox rng(kp.seed, L.id, static_cast<uint32_t>(step));
-            maybe_scatter(L.s, L.I, kp.albedo, fabs(L.dl), kp.length_scale, fs, kp.a, kp.M, rng);
+            ScatterState st;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) st.s[c] = L.s[c];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) st.I[q] = L.I[q];
+            if (maybe_scatter(&st, kp.albedo, fabs(L.dl), kp.length_scale, fs, kp.a, kp.M, rng)) {
+#pragma unroll
+                for (int c = 4; c < 8; ++c) L.s[c] = st.s[c];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) L.I[q] = st.I[q];
+            }
         }
     }
     if (kp.image_mode && phase0 == 2) {  // ImageForward
@@ -309,7 +350,7 @@ GRT_DEV int post_step(const KParams& kp, const double* s_r, const double* s_th, 
 }
 
 template <int INTEGRATOR, class RHS, bool RAW = false>
-GRT_DEV void trace_body(const KParams& kp, const double* s_r, const double* s_th, const double* s_ph) {
+GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     Lane L;
@@ -396,7 +437,7 @@ GRT_DEV void trace_body(const KParams& kp, const double* s_r, const double* s_th
                     rk4_step<RHS>(L.s, taken, kp, 1);
                     RHS::after_accept(L.s, kp, 1);
                     ++cnt.accepted;
-                    terminated = post_step<RAW>(kp, s_r, s_th, s_ph, L, phase0, taken,
+                    terminated = post_step<RAW>(kp, ax, L, phase0, taken,
                                            kp.step0 + L.calls - 1, tdisp, pdisp, have_disp);
                     finished = terminated;
                 } else {
@@ -405,7 +446,7 @@ GRT_DEV void trace_body(const KParams& kp, const double* s_r, const double* s_th
                     // samples next: after emission (not ImageBackward) and outside
                     // the fluid grid.  Fixed-step RK4 calls may use it everywhere.
                     L.fast = (L.phase != 1 && r * r > kp.fp32_min_radius_sq) ? 1 : 0;
-                    L.k1 = RHS::eval(L.s, kp, L.fast);
+                    L.need_k1 = 1;
                     L.dl_try = L.dl;
                     L.attempts = 0;
                     L.mid_call = 1;
@@ -414,7 +455,8 @@ GRT_DEV void trace_body(const KParams& kp, const double* s_r, const double* s_th
         }
         if (INTEGRATOR == 1 && L.mid_call) {
             const double taken = L.dl_try;
-            const int ok = rk45_attempt<RHS>(kp, L.s, &L.dl_try, L.k1, L.fast);
+            const int ok = rk45_attempt<RHS>(kp, L.s, &L.dl_try, L.k1, L.need_k1, L.fast, kk);
+            L.need_k1 = 0;
             ++L.attempts;
             if (ok) {
                 RHS::after_accept(L.s, kp, L.fast);
@@ -422,7 +464,7 @@ GRT_DEV void trace_body(const KParams& kp, const double* s_r, const double* s_th
                 L.dl = L.dl_try;
                 L.mid_call = 0;
                 const int phase0 = L.phase;
-                terminated = post_step<RAW>(kp, s_r, s_th, s_ph, L, phase0, taken,
+                terminated = post_step<RAW>(kp, ax, L, phase0, taken,
                                        kp.step0 + L.calls - 1, tdisp, pdisp, have_disp);
                 finished = terminated;
             } else {
@@ -468,25 +510,30 @@ GRT_DEV void trace_body(const KParams& kp, const double* s_r, const double* s_th
     }
 }
 
-// Stage the separable axes into shared memory (the lookup reads them every step).
-GRT_DEV void stage_axes(const KParams& kp, double* smem, const double*& s_r, const double*& s_th,
-                        const double*& s_ph) {
+// Shared-memory layout of a trace block: [k2..k5 slots (RK45)] [axes and
+// half-spans of a separable grid].  Returns the staged pointers.
+GRT_DEV void stage_grid(const KParams& kp, double* smem, int integrator, Axes& ax, KStore& kk) {
     const KGrid& G = kp.grid;
+    double* p = smem;
+    kk.base = p + threadIdx.x;
+    if (integrator == 1) p += 4 * 7 * kTraceThreads;
     if (G.available && G.separable) {
-        double* r = smem;
+        double* r = p;
         double* th = r + G.nr;
         double* ph = th + G.nth;
-        for (int q = threadIdx.x; q < G.nr; q += blockDim.x) r[q] = G.r_axis[q];
-        for (int q = threadIdx.x; q < G.nth; q += blockDim.x) th[q] = G.th_axis[q];
-        for (int q = threadIdx.x; q < G.nph; q += blockDim.x) ph[q] = G.ph_axis[q];
-        s_r = r;
-        s_th = th;
-        s_ph = ph;
+        double* rh = ph + G.nph;
+        double* thh = rh + G.nr;
+        double* phh = thh + G.nth;
+        for (int q = threadIdx.x; q < G.nr; q += blockDim.x) { r[q] = G.r_axis[q]; rh[q] = G.r_half[q]; }
+        for (int q = threadIdx.x; q < G.nth; q += blockDim.x) { th[q] = G.th_axis[q]; thh[q] = G.th_half[q]; }
+        for (int q = threadIdx.x; q < G.nph; q += blockDim.x) { ph[q] = G.ph_axis[q]; phh[q] = G.ph_half[q]; }
+        ax = Axes{r, th, ph, rh, thh, phh};
     } else {
-        s_r = s_th = s_ph = nullptr;
+        ax = Axes{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     }
     __syncthreads();
 }
+
 
 }  // namespace dev
 }  // namespace grt

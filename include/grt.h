@@ -278,7 +278,7 @@ typedef struct grt_device_grid {
  * place, with the same step-loop semantics as grt_run and the FP64 parity
  * kernel, on `stream` (a cudaStream_t, NULL = legacy default stream).
  * It creates no context, allocates nothing and frees nothing.  Its scratch
- * (work-queue head, counters, staged grid axes) is a 64 KiB array in the
+ * (work-queue head, counters, staged grid axes) is a 128 KiB array in the
  * library that each GPU loading the library holds until exit, shared by all
  * calls: serialise calls per device, because calls that overlap on the GPU
  * race on it.  Limits: nr + ntheta + nphi <= 8160 (larger grids are rejected

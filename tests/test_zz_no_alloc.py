@@ -5,7 +5,7 @@ whose device memory belongs to their own pool or a fixed budget, and loops
 that must not allocate after start-up because cudaMalloc can synchronise the
 device.  Such a caller keeps the grid and the photons in device memory it
 already owns; this entry point traces them in place, keeping its own scratch
-(work-queue head, counters, staged grid axes) in a 64 KiB array inside the
+(work-queue head, counters, staged grid axes) in a 128 KiB array inside the
 library, so it allocates nothing.
 
 Here the test (not the entry point) owns the device memory, through torch.
