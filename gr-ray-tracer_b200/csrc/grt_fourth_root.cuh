@@ -8,10 +8,11 @@
 // function returns the correctly rounded fourth root instead, so the kernels
 // and the CPU oracle agree bit for bit:
 //   y = RN(sqrt(RN(sqrt(x))))  (IEEE sqrt, identical on host and device) is
-//   within 1.5 ulp of x^(1/4); y is then moved while x lies beyond the fourth
-//   power of the rounding midpoint next to it, tested exactly in 256-bit
-//   integer arithmetic (a midpoint has 54+ significant bits, so x can never
-//   equal its fourth power: there are no ties).
+//   within 1.5 ulp of x^(1/4); a floating-point rounding test with a proven
+//   error bound settles almost every candidate, and y is otherwise moved while
+//   x lies beyond the fourth power of the rounding midpoint next to it, tested
+//   exactly in 256-bit integer arithmetic (a midpoint has 54+ significant
+//   bits, so x can never equal its fourth power: there are no ties).
 #pragma once
 
 #include <math.h>
@@ -19,8 +20,10 @@
 
 #if defined(__CUDACC__)
 #define GRT_FR_HD __host__ __device__ __forceinline__
+#define GRT_FR_SLOW static __host__ __device__ __noinline__
 #else
 #define GRT_FR_HD inline
+#define GRT_FR_SLOW inline
 #endif
 
 namespace grt {
@@ -124,8 +127,9 @@ GRT_FR_HD void decompose(double v, uint64_t& m, int& e) {
 
 }  // namespace fr
 
-// Correctly rounded (to nearest) x^(1/4) for x >= 0.
-GRT_FR_HD double fourth_root_cr(double x) {
+// Correctly rounded (to nearest) x^(1/4) for x >= 0 by the exact midpoint
+// test alone (the fallback of fourth_root_cr).
+GRT_FR_SLOW double fourth_root_exact(double x) {
     if (!(x > 0.0) || !(x < INFINITY)) return sqrt(sqrt(x));  // 0, inf, nan
     double y = sqrt(sqrt(x));
     uint64_t X;
@@ -151,6 +155,45 @@ GRT_FR_HD double fourth_root_cr(double x) {
         break;
     }
     return y;
+}
+
+// Correctly rounded (to nearest) x^(1/4) for x >= 0.
+//
+// Fast path (Ziv-style rounding test): for a candidate y = M 2^E that is not a
+// power of two, with u = 2^E its ulp, y is the correctly rounded root iff
+// (y - u/2)^4 < x < (y + u/2)^4.  Both gaps exceed 2 y^3 u (1 - 2^-52), so
+// |x - y^4| < 2 y^3 u (1 - 2^-42) proves y.  The residual is formed with
+// exact products (y^2 = p + pe, p^2 = q + qe by fma) and x - q exact by
+// Sterbenz's lemma; its error is below 2^-103 y^4 < 2^-51 (2 y^3 u), and the
+// computed bound 2 (p y) u (1 - 2^-40) is below 2 y^3 u (1 - 2^-41), so an
+// accepted y is always the correctly rounded one.  A residual beyond the
+// bound moves y one ulp and tests again; powers of two, inputs outside
+// [2^-900, 2^900] (where the products could leave the normal range) and
+// candidates the test cannot settle in three tries take the exact path.
+GRT_FR_HD double fourth_root_cr(double x) {
+    if (x > 0x1p-900 && x < 0x1p900) {
+        double y = sqrt(sqrt(x));
+        for (int it = 0; it < 3; ++it) {
+            const uint64_t b = fr::bits_of(y);
+            if ((b & ((1ull << 52) - 1)) == 0) break;  // power of two
+            const double u = fr::from_bits((b & (0x7FFull << 52)) - (52ull << 52));  // 2^E
+            const double p = y * y;
+            const double pe = fma(y, y, -p);
+            const double q = p * p;
+            const double qe = fma(p, p, -q);
+            const double lo = qe + (2.0 * p) * pe;
+            const double r = (x - q) - lo;
+            const double T = ((2.0 * (p * y)) * u) * (1.0 - 0x1p-40);
+            if (r > T) {
+                y = fr::from_bits(b + 1);
+            } else if (r < -T) {
+                y = fr::from_bits(b - 1);
+            } else {
+                return y;
+            }
+        }
+    }
+    return fourth_root_exact(x);
 }
 
 }  // namespace grt

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "grt.h"
+#include "grt_fourth_root.cuh"  // the product's controller root, checked below against cr::fourth_root
 #include "grt_user_physics.h"
 
 namespace oracle {
@@ -1336,6 +1337,16 @@ double oracle_philox_drand(uint64_t seed, uint64_t id, uint32_t domain, int inde
 }
 void oracle_set_pow_mode(int mode) { g_pow_mode = mode; }
 double oracle_fourth_root(double x) { return cr::fourth_root(x); }
+// Element-wise: out_oracle[i] = the oracle's arbitrary-precision root,
+// out_product[i] = the product's fourth_root_cr (rounding test + 256-bit
+// fallback) compiled for the host; the two must agree bit for bit.
+void oracle_fourth_root_pair(const double* x, uint64_t n, double* out_oracle, double* out_product) {
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < static_cast<long long>(n); ++i) {
+        out_oracle[i] = cr::fourth_root(x[i]);
+        out_product[i] = grt::fourth_root_cr(x[i]);
+    }
+}
 // Algorithmic op counts (add+sub, mul, div, sqrt, pow) of one RHS, one RK4
 // step and one RKF45 attempt (with k1 given) at the state X/P, from the
 // Counted instantiation; checks[3] = max |Counted - double| over the results.

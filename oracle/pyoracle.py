@@ -69,6 +69,8 @@ class Oracle:
         L.oracle_set_pow_mode.argtypes = [C.c_int]
         L.oracle_fourth_root.argtypes = [C.c_double]
         L.oracle_fourth_root.restype = C.c_double
+        L.oracle_fourth_root_pair.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.oracle_fourth_root_pair.restype = None
         L.oracle_observation_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint64]
         L.oracle_observation_bin.restype = C.c_uint64
 

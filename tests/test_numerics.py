@@ -44,3 +44,27 @@ def test_fourth_root_correctly_rounded(oracle):
         assert oracle.lib.oracle_fourth_root(x) == want, x
     assert oracle.lib.oracle_fourth_root(0.0) == 0.0
     assert math.isinf(oracle.lib.oracle_fourth_root(math.inf))
+
+
+def test_product_fourth_root_matches_oracle(oracle):
+    """The kernels' fourth_root_cr (rounding test with a 256-bit fallback),
+    compiled for the host, equals the oracle's arbitrary-precision root bit for
+    bit -- on random inputs over the whole range, on fourth powers of rounding
+    midpoints and their neighbours (the hardest cases), and around powers of two."""
+    rng = np.random.default_rng(1)
+    y = 10.0 ** rng.uniform(-200, 200, 500_000)
+    mids = y + np.spacing(y) / 2
+    with np.errstate(over="ignore"):
+        m4 = mids ** 4
+        cases = [m4, np.nextafter(m4, np.inf), np.nextafter(m4, 0.0), y ** 4,
+                 10.0 ** rng.uniform(-300, 300, 500_000), 10.0 ** rng.uniform(-12, 8, 500_000)]
+    p2 = np.ldexp(1.0, rng.integers(-1070, 1020, 50_000))
+    cases += [p2, np.nextafter(p2, 0.0), np.nextafter(p2, np.inf),
+              np.array([5e-324, 1e-310, 2.0 ** -1022, 2.0 ** -900, 2.0 ** 900, 1.7976931348623157e308])]
+    x = np.concatenate(cases)
+    x = np.ascontiguousarray(x[np.isfinite(x) & (x > 0)])
+    a = np.empty_like(x)
+    b = np.empty_like(x)
+    oracle.lib.oracle_fourth_root_pair(x.ctypes.data, C.c_uint64(x.size), a.ctypes.data, b.ctypes.data)
+    bad = np.flatnonzero(a.view(np.uint64) != b.view(np.uint64))
+    assert bad.size == 0, x[bad[:5]]
