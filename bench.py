@@ -7,19 +7,27 @@ Workload (default, the configuration the headline metric is quoted on):
   camera at 1000 M, inclination 17 deg, absorption and emission on.
   Synthetic inputs (the torus generator), one ray per pixel centre.
 
-A step = one pass of the hot path over the image: initialise the 65,536
-pixel rays on the device, trace them to termination (grt_run), accumulate the
-image products.  `value` is rays/s of the mixed-precision batched form with
-the grid resident in HBM; the plain FP64 form is timed the same way beside it
-and the Stokes-I error of the mixed image against the FP64 image is reported.
-`e2e` repeats the step through the C ABI with host buffers: the photon SoA is
-uploaded from pinned host memory and the image products are copied back every
-step.  L2 is flushed (a 256 MB device write) before every timed step, outside
-the events.
+Forms, each timed over the same steps:
+  fp64           the plain FP64 parity kernel, one 256x256 image per step
+                 (initialise the 65,536 pixel rays on the device, trace them
+                 to termination with grt_run, build the image products);
+  fp64_batched   the same kernel on the C2 image at four frequency channels
+                 (230/345/86/43 GHz: custom generator frequency and emission
+                 coefficient scaled by f/230 GHz) traced by ONE persistent
+                 launch, 262,144 rays per step, run as the context's CUDA
+                 graph (init + trace + every image's products);
+  mixed_batched  the mixed FP32/FP64 kernel on that batch (autotuned launch
+                 shape) -- the headline when every channel's Stokes-I image is
+                 within 1e-5 (L2 relative) of the FP64 image of that channel.
+`value` is rays/s of the headline form with the grid resident in HBM.
+`e2e` repeats the headline step through the C ABI with host buffers: the
+photon SoA is uploaded from pinned host memory and every image's products are
+copied back every step.  L2 is flushed (a 256 MB device write) before every
+timed step, outside the events.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank traces its own full image (replicas, weak scaling);
+Under torchrun each rank traces its own full batch (replicas, weak scaling);
 times are CUDA-event times, max over ranks.
 """
 
@@ -161,12 +169,12 @@ def pinned_photons(n):
     return pa
 
 
-def pinned_products(p):
+def pinned_products(p, nx, ny):
     import numpy as np
     import torch
     from grt.abi import ProductArrays
     out = ProductArrays(0, 0, 0)
-    out.nx, out.ny, out.bins = p.image_nx, p.image_ny, p.spectrum_bins
+    out.nx, out.ny, out.bins = nx, ny, p.spectrum_bins
     keep = []
 
     def mk(shape, dtype=torch.float64):
@@ -174,7 +182,7 @@ def pinned_products(p):
         keep.append(t)
         return t.numpy()
     for f in ("image_I", "image_Q", "image_U", "image_V"):
-        setattr(out, f, mk((p.image_ny, p.image_nx)))
+        setattr(out, f, mk((ny, nx)))
     out.spectrum_frequency_hz = mk((p.spectrum_bins,))
     out.spectrum_I = mk((p.spectrum_bins,))
     out.arrived_count = mk((1,), torch.int64).view(np.uint64)
@@ -198,101 +206,153 @@ def run_ours(args):
 
     world, rank, local = dist_setup(args.gpus)
     w = workloads.WORKLOADS[args.workload]
-    n_rays = w.pixels * w.pixels
+    bw = workloads.BATCHES[args.workload]
     grid = w.torus()
     stream = torch.cuda.Stream()
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
+    # Forms (all on the same torus, all through the C ABI):
+    #   fp64           -- the plain FP64 parity kernel, one image per launch
+    #                     (the reference's structure), grt_run;
+    #   fp64_batched   -- the FP64 kernel on the batch (every frequency channel
+    #                     of the image in one persistent launch), render graph;
+    #   mixed_batched  -- the mixed FP32/FP64 kernel on the batch, autotuned
+    #                     launch shape, render graph.
+    FORMS = {"fp64": (abi.PREC_FP64, False), "fp64_batched": (abi.PREC_FP64, True),
+             "mixed_batched": (abi.PREC_MIXED, True)}
+    wanted = [f for f in args.forms.split(",") if f]
     forms = {}
-    wanted = set(args.forms.split(","))
-    for name, prec in (("fp64", abi.PREC_FP64), ("mixed_batched", abi.PREC_MIXED)):
-        if name not in wanted:
-            continue
-        p = w.params()
+    for name in wanted:
+        prec, batched = FORMS[name]
+        p = (bw if batched else w).params()
         p.precision = prec
         ctx = lib.Context(p)
         ctx.set_stream(stream.cuda_stream)
         ctx.upload_grid(grid)
-        forms[name] = ctx
+        forms[name] = (ctx, batched)
+    specs = bw.specs()
 
-    def prepare(ctx):
-        ctx.init_image_photons(w.pixels, w.pixels)
+    def prepare(ctx, batched):
+        if batched:
+            ctx.init_image_batch(specs)
+        else:
+            ctx.init_image_photons(w.pixels, w.pixels)
 
-    # the batched form picks its launch shape with the autotuner; the FP64
-    # form keeps the library's default shape
-    cfg = None
-    if "mixed_batched" in forms and not args.no_autotune:
-        cfg, _, table = autotune.tune(forms["mixed_batched"], prepare, w.name, log=None)
-        for c, ms in sorted(table, key=lambda x: x[1])[:8]:
-            log(f"autotune {c} {ms:.3f} ms")
+    # the batched forms pick their launch shape with the autotuner; the plain
+    # FP64 form keeps the library's default shape
+    cfg = {}
+    for name, (ctx, batched) in forms.items():
+        if batched and not args.no_autotune:
+            cfg[name], _, table = autotune.tune(ctx, lambda c: prepare(c, True), bw.name, log=None)
+            for c, ms in sorted(table, key=lambda x: x[1])[:4]:
+                log(f"autotune {name} {c} {ms:.3f} ms")
+        else:
+            cfg[name] = ctx.launch_config()
     peak64, peak32 = lib.measure_fma_peaks()
 
-    def one_step(ctx):
+    def one_step(ctx, batched):
+        if batched:
+            st = ctx.render_graph()  # graph: init rays, trace, every image's products
+            return st, None
         ctx.init_image_photons(w.pixels, w.pixels)
         st = ctx.run()
-        prod = ctx.image_products()
-        return st, prod
+        return st, ctx.image_products()
 
     results = {}
     images = {}
     sampler = ClockSampler(local)
     with sampler:
-        for name, ctx in forms.items():
+        for name, (ctx, batched) in forms.items():
+            prepare(ctx, batched)
             for _ in range(args.warmup):
-                one_step(ctx)
+                one_step(ctx, batched)
             torch.cuda.synchronize()
             barrier(world)
             total_ms = 0.0
             trace_ms = 0.0
-            stats_acc = None
             launches = 0
+            stats_acc = None
             for _ in range(args.steps):
                 with torch.cuda.stream(stream):
                     flush_buf.zero_()
                 ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 ev0.record(stream)
-                st, prod = one_step(ctx)
+                st, prod = one_step(ctx, batched)
                 ev1.record(stream)
                 ev1.synchronize()
                 total_ms += ev0.elapsed_time(ev1)
                 trace_ms += st["trace_ms"]
-                launches += st["launches"] + 2  # init + trace launches + products
+                # our kernels per step: inits + trace launches + products
+                launches += (len(specs) if batched else 1) * 2 + st["launches"]
                 stats_acc = st
             torch.cuda.synchronize()
             barrier(world)
             total_ms = max_over_ranks(total_ms, world)
-            images[name] = prod.image_I.copy()
+            n_rays = bw.rays if batched else w.pixels * w.pixels
+            if batched:
+                images[name] = [ctx.batch_image_products(k).image_I.copy() for k in range(len(specs))]
+            else:
+                images[name] = [prod.image_I.copy()]
             results[name] = dict(ms_per_step=total_ms / args.steps, trace_ms_per_launch=trace_ms / args.steps,
-                                 stats=stats_acc, launches=launches,
+                                 stats=stats_acc, launches=launches, rays=n_rays,
                                  rays_per_s=world * n_rays * args.steps / (total_ms * 1e-3),
                                  rk_steps_per_s=world * stats_acc["accepted_steps"] * args.steps / (total_ms * 1e-3))
     clocks = sampler.summary()
 
+    # Stokes-I error of every frequency channel of the mixed batch against the
+    # FP64 image of the same channel (the FP64 batch is bitwise the FP64 form
+    # per image; without it, the channels are rendered once by the FP64 form).
     stokes_err = per_pixel = None
-    if "fp64" in images and "mixed_batched" in images:
-        ref_img = images["fp64"]
-        diff = images["mixed_batched"] - ref_img
-        nref = float(np.linalg.norm(ref_img))
-        stokes_err = float(np.linalg.norm(diff) / nref) if nref > 0 else float(np.linalg.norm(diff))
-        mask = np.abs(ref_img) > 1e-3 * np.abs(ref_img).max()
-        per_pixel = float(np.max(np.abs(diff[mask]) / np.abs(ref_img[mask]))) if mask.any() else 0.0
-    # headline form: the fastest form whose image meets the 1e-5 Stokes-I bar
-    if "mixed_batched" in results and (stokes_err is None or stokes_err <= 1e-5):
+    if "mixed_batched" in images:
+        if "fp64_batched" in images:
+            ref_imgs = images["fp64_batched"]
+        else:
+            q = bw.params()
+            ctx = lib.Context(q)
+            ctx.upload_grid(grid)
+            ctx.init_image_batch(specs)
+            ctx.run()
+            ref_imgs = [ctx.batch_image_products(k).image_I.copy() for k in range(len(specs))]
+            ctx.close()
+        errs, pix = [], []
+        for got, ref_img in zip(images["mixed_batched"], ref_imgs):
+            diff = got - ref_img
+            nref = float(np.linalg.norm(ref_img))
+            errs.append(float(np.linalg.norm(diff) / nref) if nref > 0 else float(np.linalg.norm(diff)))
+            mask = np.abs(ref_img) > 1e-3 * np.abs(ref_img).max()
+            pix.append(float(np.max(np.abs(diff[mask]) / np.abs(ref_img[mask]))) if mask.any() else 0.0)
+        stokes_err, per_pixel = max(errs), max(pix)
+    # headline form: the mixed batch when its images meet the 1e-5 Stokes-I bar
+    if "mixed_batched" in results and stokes_err is not None and stokes_err <= 1e-5:
         head = "mixed_batched"
+    elif "fp64_batched" in results:
+        head = "fp64_batched"
     else:
-        head = "fp64"
+        head = next(iter(results))
     H = results[head]
+    ctx, batched = forms[head]
 
     # ---- e2e: the C ABI with host buffers (pinned), copies inside the timed region ----
-    ctx = forms[head]
+    prepare(ctx, batched)
+    n_rays = ctx.n
     host_in = pinned_photons(n_rays)
-    ctx.init_image_photons(w.pixels, w.pixels)
     ctx.download_photons(host_in)
-    host_out = pinned_products(ctx.params)
-    for _ in range(args.warmup):
+    if batched:
+        host_out = [pinned_products(ctx.params, sp.nx, sp.ny) for sp in specs]
+    else:
+        host_out = [pinned_products(ctx.params, w.pixels, w.pixels)]
+
+    def e2e_step():
         ctx.upload_photons(host_in)
         ctx.run()
-        ctx.image_products(host_out)
+        if batched:
+            for k, out in enumerate(host_out):
+                ctx.batch_image_products(k, out)
+        else:
+            ctx.image_products(host_out[0])
+
+    for _ in range(args.warmup):
+        e2e_step()
     torch.cuda.synchronize()
     barrier(world)
     e2e_ms = 0.0
@@ -301,22 +361,21 @@ def run_ours(args):
             flush_buf.zero_()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        ctx.upload_photons(host_in)
-        ctx.run()
-        ctx.image_products(host_out)
+        e2e_step()
         ev1.record(stream)
         ev1.synchronize()
         e2e_ms += ev0.elapsed_time(ev1)
     e2e_ms = max_over_ranks(e2e_ms, world)
     p = ctx.params
-    d2h = 8 * (4 * p.image_nx * p.image_ny + p.spectrum_bins + 1)
+    d2h = sum(8 * (4 * o.nx * o.ny + p.spectrum_bins + 1) for o in host_out)
     e2e = {"value": world * n_rays * args.steps / (e2e_ms * 1e-3), "unit": "rays/s",
            "h2d_bytes_per_step": PHOTON_BYTES * n_rays, "d2h_bytes_per_step": d2h}
 
     # ---- roofline of the dominant kernel (the headline form's trace kernel) ----
-    flops = algorithmic_flops(H["stats"], w.integrator)
+    integrator = w.integrator
+    flops = algorithmic_flops(H["stats"], integrator)
     achieved = flops / (H["trace_ms_per_launch"] * 1e-3) / 1e12
-    traffic = load_traffic().get(f"{w.name}:{head}")
+    traffic = load_traffic().get(f"{bw.name if batched else w.name}:{head}")
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                 "frac": achieved / peak64, "traffic": traffic,
                 "peak_source": "measured this run: FP64 FMA microbenchmark (grt_measure_fma_peaks)",
@@ -327,8 +386,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w)
-
-    for c in forms.values():
+    for c, _ in forms.values():
         c.close()
     if rank == 0:
         line = {
@@ -345,18 +403,23 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f32+f64" if head == "mixed_batched" else "f64",
             "data": "synthetic (Fishbone-Moncrief torus generator, deterministic pixel-centre rays)",
-            "config": {"workload": w.name, "pixels": f"{w.pixels}x{w.pixels}",
+            "config": {"workload": bw.name if batched else w.name,
+                       "images": [{"inclination_deg": i, "pixels": f"{px}x{px}", "frequency_ghz": f}
+                                  for i, px, f in bw.images] if batched else None,
+                       "pixels": f"{w.pixels}x{w.pixels}",
                        "grid": "x".join(map(str, w.grid)), "spin": w.spin, "inclination_deg": w.inclination_deg,
                        "integrator": "rk45" if w.integrator else "rk4", "rtol": w.rtol,
-                       "headline_form": head, "launch": cfg,
+                       "headline_form": head, "launch": cfg.get(head),
                        "l2": "flushed by a 256 MB device write before every timed step (outside the events)",
                        "parallelism": f"replicas x{world}"},
-            "forms": {k: {"rays_per_s": v["rays_per_s"], "rk_steps_per_s": v["rk_steps_per_s"],
+            "forms": {k: {"rays_per_step": v["rays"], "rays_per_s": v["rays_per_s"],
+                          "rk_steps_per_s": v["rk_steps_per_s"],
                           "ms_per_step": v["ms_per_step"], "trace_ms_per_launch": v["trace_ms_per_launch"],
                           "accepted_steps": v["stats"]["accepted_steps"],
-                          "rejected_attempts": v["stats"]["rejected_attempts"]} for k, v in results.items()},
+                          "rejected_attempts": v["stats"]["rejected_attempts"],
+                          "launch": cfg.get(k)} for k, v in results.items()},
             "speedup_mixed_batched_vs_fp64": (results["mixed_batched"]["rays_per_s"] / results["fp64"]["rays_per_s"]
-                                              if len(results) == 2 else None),
+                                              if "mixed_batched" in results and "fp64" in results else None),
             "stokes_I_rel_err": stokes_err,
             "stokes_I_max_pixel_rel_err": per_pixel,
             "e2e": e2e,
@@ -451,7 +514,8 @@ def main():
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="use the library's default launch shape")
-    ap.add_argument("--forms", default="fp64,mixed_batched", help="comma list of fp64, mixed_batched")
+    ap.add_argument("--forms", default="fp64,fp64_batched,mixed_batched",
+                    help="comma list of fp64, fp64_batched, mixed_batched")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
     if args.impl == "reference":

@@ -8,6 +8,7 @@
 //   grt_run                integrate_geodesics step loop (integrate_cart_ks.hpp:468-527)
 //   grt_get_image_products build_observation_products (observation.hpp:31-84)
 //   grt_write_image_products_npz write_image_products (write_output.hpp:107-142)
+//   grt_init_image_batch / grt_render_graph  batched images in one launch, CUDA graph (no reference counterpart)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -116,6 +117,25 @@ struct grt_ctx {
     unsigned long long* host_u64 = nullptr;  // pinned
     grt_launch_config lc{128, 4, 1, 32};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // images of the last grt_init_image_photons (one, cameras from p) or
+    // grt_init_image_batch call; image k owns photon slots
+    // [image_start[k], image_start[k+1])
+    std::vector<grt_image_spec> images;
+    std::vector<unsigned long long> image_start;
+    uint64_t image_id_offset = 0;
+    bool batched = false;      // trace kernels read the per-image table
+    bool have_images = false;  // photons came from an image init (a render can re-initialise them)
+    DevBuf<grt::KImage> images_dev;
+    DevBuf<unsigned long long> image_start_dev;
+    // per-image products of a batch: image k's I,Q,U,V at bimage + bimage_off[k]
+    DevBuf<double> bimage, bspectrum;
+    DevBuf<unsigned long long> barrived;
+    std::vector<size_t> bimage_off;
+    bool bproducts_valid = false;
+    // render graph, valid while generation == graph_generation
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    uint64_t generation = 1, graph_generation = 0;
 };
 
 namespace {
@@ -209,8 +229,6 @@ grt::KParams make_kparams(const grt_ctx* c) {
     k.min_scale = p.min_step_scale;
     k.max_scale = p.max_step_scale;
     k.safety = p.safety;
-    k.kappa = p.absorption_coefficient;
-    k.jcoef = p.emission_coefficient;
     k.albedo = p.scattering_albedo;
     k.length_scale = p.length_cm_per_code;
     k.time_scale = p.time_s_per_code;
@@ -221,7 +239,6 @@ grt::KParams make_kparams(const grt_ctx* c) {
     k.pl_slope = p.power_law_slope;
     k.nu_min = p.nu_min_hz;
     k.nu_max = p.nu_max_hz;
-    k.nu_custom = p.custom_frequency_hz;
     k.seed = p.scattering_seed + static_cast<uint64_t>(p.rank);
     k.integrator = p.integrator;
     k.image_mode = p.mode == GRT_MODE_IMAGE;
@@ -231,18 +248,9 @@ grt::KParams make_kparams(const grt_ctx* c) {
     k.scat_on = p.scattering_enabled && c->fluid_available;
     k.generator = p.generator;
     // camera_plane_crossing basis (integrate_cart_ks.hpp:97-107), host libm.
-    k.cam_D = p.camera_distance;
-    k.cam_W = p.camera_width;
-    k.cam_H = p.camera_height;
-    k.cam_n[0] = std::sin(p.camera_theta) * std::cos(p.camera_phi);
-    k.cam_n[1] = std::sin(p.camera_theta) * std::sin(p.camera_phi);
-    k.cam_n[2] = std::cos(p.camera_theta);
-    k.cam_th[0] = std::cos(p.camera_theta) * std::cos(p.camera_phi);
-    k.cam_th[1] = std::cos(p.camera_theta) * std::sin(p.camera_phi);
-    k.cam_th[2] = -std::sin(p.camera_theta);
-    k.cam_ph[0] = -std::sin(p.camera_phi);
-    k.cam_ph[1] = std::cos(p.camera_phi);
-    k.cam_ph[2] = 0.0;
+    k.img0 = grt::make_kimage(p.camera_theta, p.camera_phi, p.camera_distance, p.camera_width,
+                                p.camera_height, p.custom_frequency_hz, p.absorption_coefficient,
+                                p.emission_coefficient);
     grt::KGrid& g = k.grid;
     g.nr = c->nr;
     g.nth = c->nth;
@@ -263,6 +271,11 @@ grt::KParams make_kparams(const grt_ctx* c) {
     g.mag = c->mag.ptr;
     g.r_reject_lo = c->r_reject_lo;
     g.r_reject_hi = c->r_reject_hi;
+    if (c->batched) {
+        k.images = c->images_dev.ptr;
+        k.image_start = c->image_start_dev.ptr;
+        k.nimages = static_cast<int>(c->images.size());
+    }
     k.ph = c->ph.view();
     k.n = c->n;
     k.counters = c->counters.ptr;
@@ -326,6 +339,10 @@ void grt_destroy(grt_ctx* c) {
     c->ph.release();
     c->counters.release();
     c->image.release(); c->spectrum.release(); c->arrived.release(); c->scratch_u64.release();
+    c->images_dev.release(); c->image_start_dev.release();
+    c->bimage.release(); c->bspectrum.release(); c->barrived.release();
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
     if (c->host_counters) cudaFreeHost(c->host_counters);
     if (c->host_u64) cudaFreeHost(c->host_u64);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -339,12 +356,14 @@ grt_status grt_set_params(grt_ctx* c, const grt_params* p) {
     char buf[512];
     if (grt_params_validate(p, buf, sizeof(buf)) != GRT_OK) return fail(c, GRT_EINVAL, buf);
     c->p = *p;
+    ++c->generation;
     return GRT_OK;
 }
 
 grt_status grt_set_stream(grt_ctx* c, void* stream) {
     if (!c) return GRT_EINVAL;
     c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+    ++c->generation;
     return GRT_OK;
 }
 
@@ -371,6 +390,7 @@ grt_status grt_set_launch_config(grt_ctx* c, const grt_launch_config* cfg) {
     if (cfg->photons_per_grab < 1 || cfg->photons_per_grab > (1 << 20))
         return fail(c, GRT_EINVAL, "photons_per_grab must be in [1, 2^20]");
     c->lc = *cfg;
+    ++c->generation;
     return GRT_OK;
 }
 
@@ -379,6 +399,7 @@ grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const 
                            const double* mag4) {
     if (!c) return GRT_EINVAL;
     const size_t ncell = nr * nth * nph;
+    ++c->generation;
     c->grid_uploaded = true;
     c->fluid_available = false;
     c->separable = false;
@@ -506,8 +527,17 @@ static grt_status count_initial_terminated(grt_ctx* c) {
 grt_status grt_upload_photons(grt_ctx* c, const grt_photon_soa* s, size_t n) {
     if (!c || (!s && n)) return GRT_EINVAL;
     if (n > (1ull << 40)) return fail(c, GRT_EINVAL, "photon count too large");
+    const bool keep_images = c->have_images && n == c->n;  // same slots: photons keep their images
     GRT_CUDA(c, c->ph.alloc(n), "alloc photons");
     c->n = n;
+    c->bproducts_valid = false;
+    if (!keep_images) {
+        ++c->generation;
+        c->images.clear();
+        c->image_start.clear();
+        c->batched = false;
+        c->have_images = false;
+    }
     if (n == 0) {
         c->initial_terminated = 0;
         return GRT_OK;
@@ -542,35 +572,246 @@ grt_status grt_download_photons(grt_ctx* c, grt_photon_soa* s) {
     return GRT_OK;
 }
 
-grt_status grt_init_image_photons(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t id_offset) {
-    if (!c) return GRT_EINVAL;
-    const size_t n = static_cast<size_t>(nx * ny);
-    GRT_CUDA(c, c->ph.alloc(n), "alloc photons");
-    c->n = n;
-    c->initial_terminated = 0;
+}  // extern "C"
+
+namespace {
+
+grt_image_spec spec_from_params(const grt_params& p, uint64_t nx, uint64_t ny) {
+    grt_image_spec sp;
+    sp.camera_theta = p.camera_theta;
+    sp.camera_phi = p.camera_phi;
+    sp.camera_distance = p.camera_distance;
+    sp.camera_width = p.camera_width;
+    sp.camera_height = p.camera_height;
+    sp.nx = nx;
+    sp.ny = ny;
+    sp.custom_frequency_hz = p.custom_frequency_hz;
+    sp.absorption_coefficient = p.absorption_coefficient;
+    sp.emission_coefficient = p.emission_coefficient;
+    return sp;
+}
+
+// initialize_photons_image (initialize_photons.hpp:82-170) for every image of
+// the context's image set, pixel-centre screen points.
+grt_status launch_image_inits(grt_ctx* c) {
     const grt_params& p = c->p;
-    grt::InitImageArgs a;
+    for (size_t k = 0; k < c->images.size(); ++k) {
+        const grt_image_spec& sp = c->images[k];
+        grt::InitImageArgs a;
+        a.ph = c->ph.view();
+        a.offset = c->image_start[k];
+        a.nx = sp.nx;
+        a.ny = sp.ny;
+        a.id_offset = c->image_id_offset + c->image_start[k];
+        a.W = sp.camera_width;
+        a.H = sp.camera_height;
+        // initialize_photons.hpp:94-108, evaluated on the host exactly as there.
+        a.cx = sp.camera_distance * std::sin(sp.camera_theta) * std::cos(sp.camera_phi);
+        a.cy = sp.camera_distance * std::sin(sp.camera_theta) * std::sin(sp.camera_phi);
+        a.cz = sp.camera_distance * std::cos(sp.camera_theta);
+        a.th_hat[0] = std::cos(sp.camera_theta) * std::cos(sp.camera_phi);
+        a.th_hat[1] = std::cos(sp.camera_theta) * std::sin(sp.camera_phi);
+        a.th_hat[2] = -std::sin(sp.camera_theta);
+        a.ph_hat[0] = -std::sin(sp.camera_phi);
+        a.ph_hat[1] = std::cos(sp.camera_phi);
+        a.ph_hat[2] = 0.0;
+        a.a = p.spin;
+        a.M = p.mass;
+        a.dlambda0 = p.initial_step * sp.camera_distance;
+        GRT_CUDA(c, grt::launch_init_image(a, c->stream), "init_image_pixels");
+    }
+    return GRT_OK;
+}
+
+grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages, uint64_t id_offset, bool batched) {
+    unsigned long long total = 0;
+    std::vector<unsigned long long> start(nimages + 1, 0);
+    for (size_t k = 0; k < nimages; ++k) {
+        const grt_image_spec& sp = specs[k];
+        if (sp.nx == 0 || sp.ny == 0 || sp.nx > (1u << 20) || sp.ny > (1u << 20))
+            return fail(c, GRT_EINVAL, "image " + std::to_string(k) + ": nx and ny must be in [1, 2^20]");
+        if (!(sp.camera_distance > 0.0) || !(sp.camera_width > 0.0) || !(sp.camera_height > 0.0) ||
+            !std::isfinite(sp.camera_theta) || !std::isfinite(sp.camera_phi))
+            return fail(c, GRT_EINVAL, "image " + std::to_string(k) +
+                                           ": camera distance, width and height must be positive and angles finite");
+        start[k] = total;
+        total += sp.nx * sp.ny;
+        if (total > (1ull << 40)) return fail(c, GRT_EINVAL, "photon count too large");
+    }
+    start[nimages] = total;
+    GRT_CUDA(c, c->ph.alloc(total), "alloc photons");
+    ++c->generation;
+    c->n = total;
+    c->initial_terminated = 0;
+    c->images.assign(specs, specs + nimages);
+    c->image_start = start;
+    c->image_id_offset = id_offset;
+    c->batched = batched;
+    c->have_images = true;
+    c->bproducts_valid = false;
+    if (batched) {
+        const grt_params& p = c->p;
+        std::vector<grt::KImage> tab(nimages);
+        for (size_t k = 0; k < nimages; ++k) {
+            const grt_image_spec& sp = specs[k];
+            tab[k] = grt::make_kimage(sp.camera_theta, sp.camera_phi, sp.camera_distance, sp.camera_width,
+                                      sp.camera_height, sp.custom_frequency_hz, sp.absorption_coefficient,
+                                      sp.emission_coefficient);
+        }
+        (void)p;
+        GRT_CUDA(c, c->images_dev.alloc(nimages), "alloc image table");
+        GRT_CUDA(c, c->image_start_dev.alloc(nimages + 1), "alloc image table");
+        GRT_CUDA(c, cudaMemcpy(c->images_dev.ptr, tab.data(), nimages * sizeof(grt::KImage), cudaMemcpyHostToDevice),
+                 "H2D image table");
+        GRT_CUDA(c, cudaMemcpy(c->image_start_dev.ptr, start.data(), (nimages + 1) * sizeof(unsigned long long),
+                               cudaMemcpyHostToDevice), "H2D image table");
+    }
+    return launch_image_inits(c);
+}
+
+// build_observation_products (observation.hpp:31-84) for photon slots
+// [offset, offset + n) into device buffers.
+grt_status launch_products(grt_ctx* c, unsigned long long offset, unsigned long long n, uint64_t nx, uint64_t ny,
+                           double W, double H, double* image, double* spectrum, unsigned long long* arrived) {
+    const grt_params& p = c->p;
+    const size_t npix = nx * ny, bins = p.spectrum_bins;
+    GRT_CUDA(c, cudaMemsetAsync(image, 0, 4 * npix * sizeof(double), c->stream), "memset");
+    GRT_CUDA(c, cudaMemsetAsync(spectrum, 0, bins * sizeof(double), c->stream), "memset");
+    GRT_CUDA(c, cudaMemsetAsync(arrived, 0, sizeof(unsigned long long), c->stream), "memset");
+    grt::ProductsArgs a;
     a.ph = c->ph.view();
-    a.offset = 0;
+    a.offset = offset;
+    a.n = n;
     a.nx = nx;
     a.ny = ny;
-    a.id_offset = id_offset;
-    a.W = p.camera_width;
-    a.H = p.camera_height;
-    // initialize_photons.hpp:94-108, evaluated on the host exactly as there.
-    a.cx = p.camera_distance * std::sin(p.camera_theta) * std::cos(p.camera_phi);
-    a.cy = p.camera_distance * std::sin(p.camera_theta) * std::sin(p.camera_phi);
-    a.cz = p.camera_distance * std::cos(p.camera_theta);
-    a.th_hat[0] = std::cos(p.camera_theta) * std::cos(p.camera_phi);
-    a.th_hat[1] = std::cos(p.camera_theta) * std::sin(p.camera_phi);
-    a.th_hat[2] = -std::sin(p.camera_theta);
-    a.ph_hat[0] = -std::sin(p.camera_phi);
-    a.ph_hat[1] = std::cos(p.camera_phi);
-    a.ph_hat[2] = 0.0;
-    a.a = p.spin;
-    a.M = p.mass;
-    a.dlambda0 = p.initial_step * p.camera_distance;
-    GRT_CUDA(c, grt::launch_init_image(a, c->stream), "init_image_pixels");
+    a.bins = bins;
+    a.W = W;
+    a.H = H;
+    a.spec_min = p.spectrum_min_hz;
+    a.spec_max = p.spectrum_max_hz;
+    a.log_min = std::log10(p.spectrum_min_hz);
+    a.log_max = std::log10(p.spectrum_max_hz);
+    a.image = image;
+    a.spectrum = spectrum;
+    a.arrived = arrived;
+    GRT_CUDA(c, grt::launch_image_products(a, c->stream), "image_products");
+    return GRT_OK;
+}
+
+// Products of every image of the image set into the per-image device buffers.
+grt_status launch_all_products(grt_ctx* c) {
+    const size_t nimg = c->images.size(), bins = c->p.spectrum_bins;
+    c->bimage_off.assign(nimg + 1, 0);
+    for (size_t k = 0; k < nimg; ++k) c->bimage_off[k + 1] = c->bimage_off[k] + 4 * c->images[k].nx * c->images[k].ny;
+    GRT_CUDA(c, c->bimage.alloc(c->bimage_off[nimg]), "alloc products");
+    GRT_CUDA(c, c->bspectrum.alloc(nimg * bins), "alloc products");
+    GRT_CUDA(c, c->barrived.alloc(nimg), "alloc products");
+    for (size_t k = 0; k < nimg; ++k) {
+        const grt_image_spec& sp = c->images[k];
+        grt_status st = launch_products(c, c->image_start[k], c->image_start[k + 1] - c->image_start[k], sp.nx, sp.ny,
+                                        sp.camera_width, sp.camera_height, c->bimage.ptr + c->bimage_off[k],
+                                        c->bspectrum.ptr + k * bins, c->barrived.ptr + k);
+        if (st != GRT_OK) return st;
+    }
+    return GRT_OK;
+}
+
+// observation.hpp:51-58, on the host like the reference.
+void fill_spectrum_frequencies(const grt_params& p, double* out) {
+    const size_t bins = p.spectrum_bins;
+    const double log_min = std::log10(p.spectrum_min_hz), log_max = std::log10(p.spectrum_max_hz);
+    for (size_t b = 0; b < bins; ++b) {
+        const double f = bins > 1 ? static_cast<double>(b) / static_cast<double>(bins - 1) : 0.0;
+        out[b] = std::pow(10.0, log_min + f * (log_max - log_min));
+    }
+}
+
+// Per-warp loop limit of a trace launch (GRT_ETIMEOUT beyond it): every
+// photon may take `budget` calls of at most 13 attempts each.
+unsigned long long iteration_limit(const grt::KParams& kp, unsigned long long total, int blocks, int threads) {
+    const unsigned long long warps = static_cast<unsigned long long>(blocks) * (threads / 32);
+    return static_cast<unsigned long long>(kp.budget + 2) * 13ull *
+               ((total + warps - 1) / warps + static_cast<unsigned long long>(kp.grab)) +
+           (1ull << 20);
+}
+
+cudaError_t launch_trace(const grt_ctx* c, const grt::KParams& kp, size_t smem) {
+    const grt_params& p = c->p;
+    return p.precision == GRT_PREC_MIXED
+               ? grt::launch_trace_mixed(kp, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream)
+               : grt::launch_trace_fp64(kp, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+}
+
+size_t trace_smem(const grt_ctx* c) {
+    return grt::dev_trace_smem_bytes(c->p.integrator, 128, c->fluid_available && c->separable, c->nr, c->nth, c->nph);
+}
+
+// steps_done of a single-launch run (termination_percent = 1): the reference
+// stops after the first output step at or after the last termination.
+int64_t single_launch_steps_done(const grt_params& p, unsigned long long terminated, unsigned long long total,
+                                 unsigned long long max_term_step) {
+    if (terminated < total) return p.max_steps;
+    const uint64_t interval = p.output_interval ? p.output_interval : 1;
+    const int64_t last = max_term_step ? static_cast<int64_t>(max_term_step) - 1 : 0;
+    int64_t s_out = static_cast<int64_t>(((static_cast<uint64_t>(last) + interval - 1) / interval) * interval);
+    if (s_out > p.max_steps - 1) s_out = p.max_steps - 1;
+    return s_out + 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+grt_status grt_init_image_photons(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t id_offset) {
+    if (!c) return GRT_EINVAL;
+    const grt_image_spec sp = spec_from_params(c->p, nx, ny);
+    if (nx * ny == 0) {
+        GRT_CUDA(c, c->ph.alloc(0), "alloc photons");
+        c->n = 0;
+        c->images.clear();
+        c->image_start.clear();
+        c->batched = false;
+        c->have_images = false;
+        ++c->generation;
+        return GRT_OK;
+    }
+    return set_image_set(c, &sp, 1, id_offset, false);
+}
+
+grt_status grt_init_image_batch(grt_ctx* c, const grt_image_spec* specs, size_t nimages, uint64_t id_offset) {
+    if (!c) return GRT_EINVAL;
+    if (!specs || nimages == 0) return fail(c, GRT_EINVAL, "an image batch needs at least one image");
+    if (nimages > (1u << 20)) return fail(c, GRT_EINVAL, "too many images in one batch");
+    return set_image_set(c, specs, nimages, id_offset, true);
+}
+
+size_t grt_batch_image_count(const grt_ctx* c) { return c && c->batched ? c->images.size() : 0; }
+
+grt_status grt_get_batch_image_products(grt_ctx* c, size_t image, grt_image_products* out) {
+    if (!c || !out) return GRT_EINVAL;
+    if (!c->batched) return fail(c, GRT_ESTATE, "no image batch (grt_init_image_batch)");
+    if (image >= c->images.size()) return fail(c, GRT_EINVAL, "image index out of range");
+    if (!out->image_I || !out->image_Q || !out->image_U || !out->image_V || !out->spectrum_frequency_hz ||
+        !out->spectrum_I || !out->arrived_count)
+        return fail(c, GRT_EINVAL, "null image product buffer");
+    if (!c->bproducts_valid) {
+        grt_status st = launch_all_products(c);
+        if (st != GRT_OK) return st;
+        c->bproducts_valid = true;
+    }
+    const grt_image_spec& sp = c->images[image];
+    const size_t npix = sp.nx * sp.ny, bins = c->p.spectrum_bins;
+    const double* src = c->bimage.ptr + c->bimage_off[image];
+    double* dst[4] = {out->image_I, out->image_Q, out->image_U, out->image_V};
+    for (int q = 0; q < 4; ++q)
+        GRT_CUDA(c, cudaMemcpyAsync(dst[q], src + q * npix, npix * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                 "D2H image");
+    GRT_CUDA(c, cudaMemcpyAsync(out->spectrum_I, c->bspectrum.ptr + image * bins, bins * sizeof(double),
+                                cudaMemcpyDeviceToHost, c->stream), "D2H spectrum");
+    GRT_CUDA(c, cudaMemcpyAsync(out->arrived_count, c->barrived.ptr + image, sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, c->stream), "D2H arrived");
+    fill_spectrum_frequencies(c->p, out->spectrum_frequency_hz);
+    GRT_CUDA(c, cudaStreamSynchronize(c->stream), "products");
     return GRT_OK;
 }
 
@@ -580,6 +821,7 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
     const grt_params& p = c->p;
     grt_run_stats st;
     std::memset(&st, 0, sizeof(st));
+    c->bproducts_valid = false;
     if (c->n == 0) {
         st.steps_done = p.max_steps;
         if (stats) *stats = st;
@@ -587,8 +829,7 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
     }
     grt::KParams kp = make_kparams(c);
     const int threads = 128;
-    const size_t smem = grt::dev_trace_smem_bytes(p.integrator, threads, c->fluid_available && c->separable, c->nr,
-                                                  c->nth, c->nph);
+    const size_t smem = trace_smem(c);
     const int blocks = c->sm_count * c->lc.blocks_per_sm;
     const unsigned long long total = c->n;
     unsigned long long terminated = c->initial_terminated;
@@ -615,15 +856,10 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
         }
         kp.step0 = step;
         kp.budget = end - step;
-        const unsigned long long warps = static_cast<unsigned long long>(blocks) * (threads / 32);
-        kp.max_iterations = static_cast<unsigned long long>(kp.budget + 2) * 13ull *
-                                ((total + warps - 1) / warps + static_cast<unsigned long long>(kp.grab)) +
-                            (1ull << 20);
+        kp.max_iterations = iteration_limit(kp, total, blocks, threads);
         GRT_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, sizeof(grt::KCounters), c->stream), "memset counters");
         GRT_CUDA(c, cudaEventRecord(c->ev0, c->stream), "event");
-        cudaError_t e = p.precision == GRT_PREC_MIXED
-                            ? grt::launch_trace_mixed(kp, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream)
-                            : grt::launch_trace_fp64(kp, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+        cudaError_t e = launch_trace(c, kp, smem);
         if (e != cudaSuccess) return cuda_fail(c, e, "trace launch");
         GRT_CUDA(c, cudaEventRecord(c->ev1, c->stream), "event");
         GRT_CUDA(c, cudaMemcpyAsync(c->host_counters, c->counters.ptr, sizeof(grt::KCounters), cudaMemcpyDeviceToHost,
@@ -651,16 +887,85 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
         const double fraction = static_cast<double>(terminated) / static_cast<double>(total);
         if (fraction >= p.termination_percent) break;
     }
-    if (single && terminated >= total) {
-        // The reference stops after the first output step at or after the last termination.
-        const int64_t last = max_term_step ? static_cast<int64_t>(max_term_step) - 1 : 0;
-        int64_t s_out = static_cast<int64_t>(((static_cast<uint64_t>(last) + interval - 1) / interval) * interval);
-        if (s_out > p.max_steps - 1) s_out = p.max_steps - 1;
-        steps_done = s_out + 1;
-    }
+    if (single && terminated >= total) steps_done = single_launch_steps_done(p, terminated, total, max_term_step);
     st.steps_done = steps_done;
     st.n_terminated = terminated;
     st.trace_ms = ms_total;
+    if (stats) *stats = st;
+    return GRT_OK;
+}
+
+grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
+    if (!c) return GRT_EINVAL;
+    if (!c->grid_uploaded) return fail(c, GRT_ESTATE, "grt_render_graph before grt_upload_grid");
+    if (!c->have_images) return fail(c, GRT_ESTATE, "grt_render_graph needs grt_init_image_photons or grt_init_image_batch");
+    const grt_params& p = c->p;
+    if (!(p.termination_percent >= 1.0))
+        return fail(c, GRT_EINVAL, "grt_render_graph needs termination_percent >= 1 (one trace launch)");
+    if (!c->graph_exec || c->graph_generation != c->generation) {
+        if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+        if (c->graph) cudaGraphDestroy(c->graph);
+        c->graph_exec = nullptr;
+        c->graph = nullptr;
+        // allocations happen before the capture
+        const size_t nimg = c->images.size(), bins = p.spectrum_bins;
+        size_t pix = 0;
+        for (const auto& sp : c->images) pix += 4 * sp.nx * sp.ny;
+        GRT_CUDA(c, c->bimage.alloc(pix), "alloc products");
+        GRT_CUDA(c, c->bspectrum.alloc(nimg * bins), "alloc products");
+        GRT_CUDA(c, c->barrived.alloc(nimg), "alloc products");
+        grt::KParams kp = make_kparams(c);
+        kp.step0 = 0;
+        kp.budget = p.max_steps;
+        kp.max_iterations = iteration_limit(kp, c->n, c->sm_count * c->lc.blocks_per_sm, 128);
+        const size_t smem = trace_smem(c);
+        GRT_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed), "begin capture");
+        grt_status gs = launch_image_inits(c);
+        cudaError_t e = cudaSuccess;
+        if (gs == GRT_OK) e = cudaMemsetAsync(c->counters.ptr, 0, sizeof(grt::KCounters), c->stream);
+        // event-record nodes around the trace kernel time it inside the graph
+        if (gs == GRT_OK && e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev0, c->stream, cudaEventRecordExternal);
+        if (gs == GRT_OK && e == cudaSuccess) e = launch_trace(c, kp, smem);
+        if (gs == GRT_OK && e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev1, c->stream, cudaEventRecordExternal);
+        if (gs == GRT_OK && e == cudaSuccess) gs = launch_all_products(c);
+        if (gs == GRT_OK && e == cudaSuccess)
+            e = cudaMemcpyAsync(c->host_counters, c->counters.ptr, sizeof(grt::KCounters), cudaMemcpyDeviceToHost,
+                                c->stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(c->stream, &g);
+        if (gs != GRT_OK) {
+            if (g) cudaGraphDestroy(g);
+            return gs;
+        }
+        if (e != cudaSuccess || ee != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(c, e != cudaSuccess ? e : ee, "render graph capture");
+        }
+        c->graph = g;
+        GRT_CUDA(c, cudaGraphInstantiate(&c->graph_exec, c->graph, 0), "graph instantiate");
+        c->graph_generation = c->generation;
+    }
+    GRT_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream), "graph launch");
+    GRT_CUDA(c, cudaStreamSynchronize(c->stream), "render graph");
+    c->initial_terminated = 0;
+    c->bproducts_valid = true;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    const grt::KCounters& k = *c->host_counters;
+    grt_run_stats st;
+    std::memset(&st, 0, sizeof(st));
+    st.accepted_steps = k.accepted;
+    st.rejected_attempts = k.rejected;
+    st.photon_calls = k.calls;
+    st.launches = 1;
+    st.n_terminated = k.terminated;
+    st.trace_ms = ms;
+    st.steps_done = single_launch_steps_done(p, k.terminated, c->n, k.max_term_step);
+    if (k.timed_out) {
+        st.timed_out = 1;
+        if (stats) *stats = st;
+        return fail(c, GRT_ETIMEOUT, "trace kernel hit its iteration limit");
+    }
     if (stats) *stats = st;
     return GRT_OK;
 }
@@ -675,27 +980,9 @@ grt_status grt_get_image_products(grt_ctx* c, grt_image_products* out) {
     GRT_CUDA(c, c->image.alloc(4 * npix), "alloc image");
     GRT_CUDA(c, c->spectrum.alloc(bins), "alloc spectrum");
     GRT_CUDA(c, c->arrived.alloc(1), "alloc arrived");
-    GRT_CUDA(c, cudaMemsetAsync(c->image.ptr, 0, 4 * npix * sizeof(double), c->stream), "memset");
-    GRT_CUDA(c, cudaMemsetAsync(c->spectrum.ptr, 0, bins * sizeof(double), c->stream), "memset");
-    GRT_CUDA(c, cudaMemsetAsync(c->arrived.ptr, 0, sizeof(unsigned long long), c->stream), "memset");
-    const double log_min = std::log10(p.spectrum_min_hz), log_max = std::log10(p.spectrum_max_hz);
-    grt::ProductsArgs a;
-    a.ph = c->ph.view();
-    a.offset = 0;
-    a.n = c->n;
-    a.nx = p.image_nx;
-    a.ny = p.image_ny;
-    a.bins = bins;
-    a.W = p.camera_width;
-    a.H = p.camera_height;
-    a.spec_min = p.spectrum_min_hz;
-    a.spec_max = p.spectrum_max_hz;
-    a.log_min = log_min;
-    a.log_max = log_max;
-    a.image = c->image.ptr;
-    a.spectrum = c->spectrum.ptr;
-    a.arrived = c->arrived.ptr;
-    GRT_CUDA(c, grt::launch_image_products(a, c->stream), "image_products");
+    grt_status st = launch_products(c, 0, c->n, p.image_nx, p.image_ny, p.camera_width, p.camera_height, c->image.ptr,
+                                    c->spectrum.ptr, c->arrived.ptr);
+    if (st != GRT_OK) return st;
     double* dst[4] = {out->image_I, out->image_Q, out->image_U, out->image_V};
     for (int q = 0; q < 4; ++q)
         GRT_CUDA(c, cudaMemcpyAsync(dst[q], c->image.ptr + q * npix, npix * sizeof(double), cudaMemcpyDeviceToHost,
@@ -704,14 +991,50 @@ grt_status grt_get_image_products(grt_ctx* c, grt_image_products* out) {
                                 c->stream), "D2H spectrum");
     GRT_CUDA(c, cudaMemcpyAsync(out->arrived_count, c->arrived.ptr, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                 c->stream), "D2H arrived");
-    // observation.hpp:51-58, on the host like the reference.
-    for (size_t b = 0; b < bins; ++b) {
-        const double f = bins > 1 ? static_cast<double>(b) / static_cast<double>(bins - 1) : 0.0;
-        out->spectrum_frequency_hz[b] = std::pow(10.0, log_min + f * (log_max - log_min));
-    }
+    fill_spectrum_frequencies(p, out->spectrum_frequency_hz);
     GRT_CUDA(c, cudaStreamSynchronize(c->stream), "products");
     return GRT_OK;
 }
+
+}  // extern "C"
+
+namespace {
+
+// write_image_products (write_output.hpp:107-142): one archive, written to a
+// temporary name and renamed into place.
+grt_status write_products_archive(grt_ctx* c, const std::string& output_dir, const std::string& file, size_t nx,
+                                  size_t ny, size_t bins, const grt_image_products& out) {
+    namespace fs = std::filesystem;
+    std::error_code ec;
+    fs::create_directories(output_dir, ec);
+    const fs::path final_path = fs::path(output_dir) / file;
+    const fs::path tmp = final_path.string() + ".tmp";
+    grt::NpzOut z;
+    if (!z.open(tmp.string())) return fail(c, GRT_EIO, "Failed to open output NumPy archive: " + tmp.string());
+    const std::vector<size_t> img{ny, nx}, spec{bins}, one{1};
+    bool ok = z.add("image_I", grt::npy_bytes("<f8", img, out.image_I, 8)) &&
+              z.add("image_Q", grt::npy_bytes("<f8", img, out.image_Q, 8)) &&
+              z.add("image_U", grt::npy_bytes("<f8", img, out.image_U, 8)) &&
+              z.add("image_V", grt::npy_bytes("<f8", img, out.image_V, 8)) &&
+              z.add("spectrum_frequency_hz", grt::npy_bytes("<f8", spec, out.spectrum_frequency_hz, 8)) &&
+              z.add("spectrum_I", grt::npy_bytes("<f8", spec, out.spectrum_I, 8)) &&
+              z.add("arrived_count", grt::npy_bytes("<u8", one, out.arrived_count, 8));
+    ok = z.close() && ok;
+    if (!ok) {
+        fs::remove(tmp, ec);
+        return fail(c, GRT_EIO, "Failed while writing NumPy archive");
+    }
+    fs::rename(tmp, final_path, ec);
+    if (ec) {
+        fs::remove(tmp, ec);
+        return fail(c, GRT_EIO, "Failed to publish output archive " + final_path.string());
+    }
+    return GRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
 
 grt_status grt_write_image_products_npz(grt_ctx* c, const char* output_dir, const char* name) {
     if (!c || !output_dir || !name) return GRT_EINVAL;
@@ -722,30 +1045,24 @@ grt_status grt_write_image_products_npz(grt_ctx* c, const char* output_dir, cons
     grt_image_products out{I.data(), Q.data(), U.data(), V.data(), sf.data(), si.data(), &arrived};
     grt_status s = grt_get_image_products(c, &out);
     if (s != GRT_OK) return s;
-    namespace fs = std::filesystem;
-    std::error_code ec;
-    fs::create_directories(output_dir, ec);
-    const fs::path final_path = fs::path(output_dir) / (std::string(name) + "_image_products.npz");
-    const fs::path tmp = final_path.string() + ".tmp";
-    grt::NpzOut z;
-    if (!z.open(tmp.string())) return fail(c, GRT_EIO, "Failed to open output NumPy archive: " + tmp.string());
-    const std::vector<size_t> img{ny, nx}, spec{bins}, one{1};
-    bool ok = z.add("image_I", grt::npy_bytes("<f8", img, I.data(), 8)) &&
-              z.add("image_Q", grt::npy_bytes("<f8", img, Q.data(), 8)) &&
-              z.add("image_U", grt::npy_bytes("<f8", img, U.data(), 8)) &&
-              z.add("image_V", grt::npy_bytes("<f8", img, V.data(), 8)) &&
-              z.add("spectrum_frequency_hz", grt::npy_bytes("<f8", spec, sf.data(), 8)) &&
-              z.add("spectrum_I", grt::npy_bytes("<f8", spec, si.data(), 8)) &&
-              z.add("arrived_count", grt::npy_bytes("<u8", one, &arrived, 8));
-    ok = z.close() && ok;
-    if (!ok) {
-        fs::remove(tmp, ec);
-        return fail(c, GRT_EIO, "Failed while writing NumPy archive");
-    }
-    fs::rename(tmp, final_path, ec);
-    if (ec) {
-        fs::remove(tmp, ec);
-        return fail(c, GRT_EIO, "Failed to publish output archive " + final_path.string());
+    return write_products_archive(c, output_dir, std::string(name) + "_image_products.npz", nx, ny, bins, out);
+}
+
+grt_status grt_write_batch_products_npz(grt_ctx* c, const char* output_dir, const char* name) {
+    if (!c || !output_dir || !name) return GRT_EINVAL;
+    if (!c->batched) return fail(c, GRT_ESTATE, "no image batch (grt_init_image_batch)");
+    const size_t bins = c->p.spectrum_bins;
+    for (size_t k = 0; k < c->images.size(); ++k) {
+        const size_t nx = c->images[k].nx, ny = c->images[k].ny;
+        std::vector<double> I(nx * ny), Q(nx * ny), U(nx * ny), V(nx * ny), sf(bins), si(bins);
+        uint64_t arrived = 0;
+        grt_image_products out{I.data(), Q.data(), U.data(), V.data(), sf.data(), si.data(), &arrived};
+        grt_status s = grt_get_batch_image_products(c, k, &out);
+        if (s != GRT_OK) return s;
+        s = write_products_archive(c, output_dir,
+                                   std::string(name) + "_image" + std::to_string(k) + "_image_products.npz", nx, ny,
+                                   bins, out);
+        if (s != GRT_OK) return s;
     }
     return GRT_OK;
 }

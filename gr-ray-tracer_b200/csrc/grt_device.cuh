@@ -478,15 +478,15 @@ static __device__ __noinline__ bool generate_power_law(Philox& rng, int packets,
 // ---------------------------------------------------------------------------
 // Camera (integrate_cart_ks.hpp:96-130); the plane basis is precomputed on the host.
 // ---------------------------------------------------------------------------
-GRT_DEV int camera_crossing(const KParams& kp, const double s[8], double& u, double& v) {
-    const double pc = s[1] * kp.cam_n[0] + s[2] * kp.cam_n[1] + s[3] * kp.cam_n[2];
-    if (pc < kp.cam_D) return 0;
-    const double rel0 = s[1] - kp.cam_D * kp.cam_n[0];
-    const double rel1 = s[2] - kp.cam_D * kp.cam_n[1];
-    const double rel2 = s[3] - kp.cam_D * kp.cam_n[2];
-    u = rel0 * kp.cam_th[0] + rel1 * kp.cam_th[1] + rel2 * kp.cam_th[2];
-    v = rel0 * kp.cam_ph[0] + rel1 * kp.cam_ph[1] + rel2 * kp.cam_ph[2];
-    const bool inside = fabs(u) <= 0.5 * kp.cam_W && fabs(v) <= 0.5 * kp.cam_H;
+GRT_DEV int camera_crossing(const KImage& im, const double s[8], double& u, double& v) {
+    const double pc = s[1] * im.cam_n[0] + s[2] * im.cam_n[1] + s[3] * im.cam_n[2];
+    if (pc < im.cam_D) return 0;
+    const double rel0 = s[1] - im.cam_D * im.cam_n[0];
+    const double rel1 = s[2] - im.cam_D * im.cam_n[1];
+    const double rel2 = s[3] - im.cam_D * im.cam_n[2];
+    u = rel0 * im.cam_th[0] + rel1 * im.cam_th[1] + rel2 * im.cam_th[2];
+    v = rel0 * im.cam_ph[0] + rel1 * im.cam_ph[1] + rel2 * im.cam_ph[2];
+    const bool inside = fabs(u) <= 0.5 * im.cam_W && fabs(v) <= 0.5 * im.cam_H;
     return inside ? 1 : -1;
 }
 

@@ -67,22 +67,38 @@ struct KCounters {
     unsigned long long pad;
 };
 
+// One image of a launch: the camera plane of integrate_cart_ks.hpp:96-107
+// (basis computed on the host with libm, as the reference computes it) and
+// the image's radiative coefficients -- custom generator frequency and the
+// absorption/emission coefficients (frequency channels of a batch differ here).
+struct KImage {
+    double cam_D, cam_W, cam_H;
+    double cam_n[3], cam_th[3], cam_ph[3];
+    double nu_custom, kappa, jcoef;
+    double pad;
+};
+
 struct KParams {
     // physics
     double a, M;
     double r_min, r_max;
     double atol, rtol, min_scale, max_scale, safety;
-    double kappa, jcoef, albedo;
+    double albedo;
     double length_scale, time_scale, density_scale, temperature_scale;
-    double norm, energy, pl_slope, nu_min, nu_max, nu_custom;
+    double norm, energy, pl_slope, nu_min, nu_max;
     uint64_t seed;             // scattering.seed + rank
     int integrator;            // GRT_RK4 / GRT_RK45
     int image_mode;            // simulation.mode == image
     int abs_on, emis_on, scat_on;  // already ANDed with fluid availability
     int generator;
-    // camera plane basis (integrate_cart_ks.hpp:96-107), computed on the host
-    double cam_D, cam_W, cam_H;
-    double cam_n[3], cam_th[3], cam_ph[3];
+    // the single image of a one-image launch (nimages == 0)
+    KImage img0;
+    // batched launch: photon index q belongs to image b when
+    // image_start[b] <= q < image_start[b + 1]; nimages == 0 uses img0
+    const KImage* images;
+    const unsigned long long* image_start;  // [nimages + 1]
+    int nimages;
+    int pad_images;
     KGrid grid;
     KPhotons ph;
     uint64_t n;                // photons in the queue

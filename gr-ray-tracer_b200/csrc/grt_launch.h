@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
+
 #include "grt_kparams.h"
 
 namespace grt {
@@ -31,6 +33,29 @@ struct ProductsArgs {
     double* spectrum;              // [bins]
     unsigned long long* arrived;   // [1]
 };
+
+// Camera plane basis of integrate_cart_ks.hpp:97-107 with host libm, plus the
+// image's coefficients.
+inline KImage make_kimage(double theta, double phi, double distance, double width, double height, double nu_custom,
+                          double kappa, double jcoef) {
+    KImage im{};
+    im.cam_D = distance;
+    im.cam_W = width;
+    im.cam_H = height;
+    im.cam_n[0] = std::sin(theta) * std::cos(phi);
+    im.cam_n[1] = std::sin(theta) * std::sin(phi);
+    im.cam_n[2] = std::cos(theta);
+    im.cam_th[0] = std::cos(theta) * std::cos(phi);
+    im.cam_th[1] = std::cos(theta) * std::sin(phi);
+    im.cam_th[2] = -std::sin(theta);
+    im.cam_ph[0] = -std::sin(phi);
+    im.cam_ph[1] = std::cos(phi);
+    im.cam_ph[2] = 0.0;
+    im.nu_custom = nu_custom;
+    im.kappa = kappa;
+    im.jcoef = jcoef;
+    return im;
+}
 
 // Dynamic shared memory of a trace launch: k2..k5 slots for RK45 (4*7 doubles
 // per thread) plus the separable axes and their half-spans (2*(nr+nth+nph)).

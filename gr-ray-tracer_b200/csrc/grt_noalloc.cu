@@ -210,8 +210,6 @@ extern "C" grt_status grt_trace_device_noalloc(const grt_params* p, const grt_de
     kp.min_scale = p->min_step_scale;
     kp.max_scale = p->max_step_scale;
     kp.safety = p->safety;
-    kp.kappa = p->absorption_coefficient;
-    kp.jcoef = p->emission_coefficient;
     kp.albedo = p->scattering_albedo;
     kp.length_scale = p->length_cm_per_code;
     kp.time_scale = p->time_s_per_code;
@@ -222,7 +220,6 @@ extern "C" grt_status grt_trace_device_noalloc(const grt_params* p, const grt_de
     kp.pl_slope = p->power_law_slope;
     kp.nu_min = p->nu_min_hz;
     kp.nu_max = p->nu_max_hz;
-    kp.nu_custom = p->custom_frequency_hz;
     kp.seed = p->scattering_seed + static_cast<uint64_t>(p->rank);
     kp.integrator = p->integrator;
     kp.image_mode = p->mode == GRT_MODE_IMAGE;
@@ -230,18 +227,9 @@ extern "C" grt_status grt_trace_device_noalloc(const grt_params* p, const grt_de
     kp.emis_on = p->emission_enabled && ncell;
     kp.scat_on = p->scattering_enabled && ncell;
     kp.generator = p->generator;
-    kp.cam_D = p->camera_distance;
-    kp.cam_W = p->camera_width;
-    kp.cam_H = p->camera_height;
-    kp.cam_n[0] = std::sin(p->camera_theta) * std::cos(p->camera_phi);
-    kp.cam_n[1] = std::sin(p->camera_theta) * std::sin(p->camera_phi);
-    kp.cam_n[2] = std::cos(p->camera_theta);
-    kp.cam_th[0] = std::cos(p->camera_theta) * std::cos(p->camera_phi);
-    kp.cam_th[1] = std::cos(p->camera_theta) * std::sin(p->camera_phi);
-    kp.cam_th[2] = -std::sin(p->camera_theta);
-    kp.cam_ph[0] = -std::sin(p->camera_phi);
-    kp.cam_ph[1] = std::cos(p->camera_phi);
-    kp.cam_ph[2] = 0.0;
+    kp.img0 = grt::make_kimage(p->camera_theta, p->camera_phi, p->camera_distance, p->camera_width,
+                                p->camera_height, p->custom_frequency_hz, p->absorption_coefficient,
+                                p->emission_coefficient);
     grt::KGrid& g = kp.grid;
     g.nr = static_cast<int>(nr);
     g.nth = static_cast<int>(nth);

@@ -72,6 +72,7 @@ struct Lane {
     // RK45 call in progress
     int mid_call;
     int attempts;
+    int img;              // image of a batched launch (0 otherwise)
     int fast;             // precision hint of the current call (mixed form)
     int need_k1;          // the call's k1 = f(state) is still to be evaluated
     double dl_try;
@@ -258,9 +259,25 @@ struct LaneCounters {
 // Everything after the integration step of one call (integrate_cart_ks.hpp:307-417).
 // phase0 is the phase loaded at the start of the call.  Returns 1 if the photon
 // terminated.
+// The image a photon belongs to: the launch's only image, or the batch entry
+// whose index range holds photon index q (binary search, once per load).
+GRT_DEV int image_of_photon(const KParams& kp, long long q) {
+    if (kp.nimages <= 0) return 0;
+    int lo = 0, hi = kp.nimages - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (kp.image_start[mid] <= static_cast<unsigned long long>(q)) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+GRT_DEV const KImage& image_params(const KParams& kp, int img) { return kp.nimages > 0 ? kp.images[img] : kp.img0; }
+
 template <bool RAW = false>
 GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, double taken, int64_t step,
                       double& tdisp, double& pdisp, int& have_disp) {
+    const KImage& im = image_params(kp, L.img);
     L.radius = ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
     L.have_radius = 1;
     const bool backward = phase0 == 1;  // ImageBackward
@@ -279,7 +296,7 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
         } else if (packets > 0 && kp.generator == 1) {
             generated = generate_power_law(rng, packets, kp.pl_slope, kp.nu_min, kp.nu_max, kp.energy, nu, E);
         } else if (packets > 0) {
-            generated = GeneratePhotonsCustom(fs.fluid, rng, packets, kp.nu_custom, kp.energy, nu, E);
+            generated = GeneratePhotonsCustom(fs.fluid, rng, packets, im.nu_custom, kp.energy, nu, E);
         }
         if (generated) {
             L.freq = nu;
@@ -298,14 +315,14 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
         }
     } else if (sampled && !backward) {
         if (kp.abs_on) {
-            double dtau = ComputeOpticalDepthIncrement(fs.fluid, L.freq, taken, kp.kappa);
+            double dtau = ComputeOpticalDepthIncrement(fs.fluid, L.freq, taken, im.kappa);
             if (kp.m_abs) dtau = kp.m_abs[fs.cell] * dtau;
             const double att = exp(-dtau);
 #pragma unroll
             for (int q = 0; q < 4; ++q) L.I[q] *= att;
         }
         if (kp.emis_on) {
-            double dI = ComputeEmissivityIncrement(fs.fluid, L.freq, taken, kp.jcoef);
+            double dI = ComputeEmissivityIncrement(fs.fluid, L.freq, taken, im.jcoef);
             if (kp.m_emis) dI = kp.m_emis[fs.cell] * dI;
             L.I[0] += dI;
         }
@@ -326,7 +343,7 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
     }
     if (kp.image_mode && phase0 == 2) {  // ImageForward
         double u = 0.0, v = 0.0;
-        const int crossing = camera_crossing(kp, L.s, u, v);
+        const int crossing = camera_crossing(im, L.s, u, v);
         if (crossing > 0) {
             const double eo = camera_observer_energy(kp, L.s);
             const double ee = L.emit;
@@ -399,6 +416,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                     if (q >= 0 && !kp.ph.terminate[q]) {
                         load_photon(kp.ph, q, L);
                         L.idx = q;
+                        L.img = image_of_photon(kp, q);
                         have_disp = 0;
                     }
                 }

@@ -105,6 +105,28 @@ class LaunchConfig(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class ImageSpec(C.Structure):
+    """grt_image_spec: one image of a batched launch."""
+    _fields_ = [("camera_theta", _D), ("camera_phi", _D), ("camera_distance", _D), ("camera_width", _D),
+                ("camera_height", _D), ("nx", _U64), ("ny", _U64), ("custom_frequency_hz", _D),
+                ("absorption_coefficient", _D), ("emission_coefficient", _D)]
+
+    @classmethod
+    def from_params(cls, p: Params, nx: int, ny: int, **kw) -> "ImageSpec":
+        sp = cls(camera_theta=p.camera_theta, camera_phi=p.camera_phi, camera_distance=p.camera_distance,
+                 camera_width=p.camera_width, camera_height=p.camera_height, nx=nx, ny=ny,
+                 custom_frequency_hz=p.custom_frequency_hz, absorption_coefficient=p.absorption_coefficient,
+                 emission_coefficient=p.emission_coefficient)
+        for k, v in kw.items():
+            if not hasattr(sp, k):
+                raise AttributeError(f"grt_image_spec has no field {k!r}")
+            setattr(sp, k, v)
+        return sp
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 def _ptr(arr, ctype):
     return arr.ctypes.data_as(C.POINTER(ctype))
 

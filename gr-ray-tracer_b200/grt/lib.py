@@ -14,8 +14,8 @@ from pathlib import Path
 
 import numpy as np
 
-from .abi import (GRT_OK, STATUS_NAMES, DeviceGrid, ImageProducts, LaunchConfig, Params, PhotonArrays,
-                  PhotonSoA, ProductArrays, RunStats)
+from .abi import (GRT_OK, STATUS_NAMES, DeviceGrid, ImageProducts, ImageSpec, LaunchConfig, Params,
+                  PhotonArrays, PhotonSoA, ProductArrays, RunStats)
 
 PKG_ROOT = Path(__file__).resolve().parent.parent
 LIB_PATH = PKG_ROOT / "lib" / "libgrt_b200.so"
@@ -77,7 +77,14 @@ def load(path: Path | None = None):
     L.grt_measure_fma_peaks.argtypes = [P(C.c_double), P(C.c_double)]
     L.grt_trace_device_noalloc.argtypes = [P(Params), P(DeviceGrid), P(PhotonSoA), C.c_uint64, P(RunStats),
                                            vp, C.c_char_p, C.c_size_t]
-    for name in ("grt_trace_device_noalloc", "grt_measure_fma_peaks", "grt_params_validate", "grt_params_from_toml", "grt_create", "grt_set_params",
+    L.grt_init_image_batch.argtypes = [vp, P(ImageSpec), C.c_size_t, C.c_uint64]
+    L.grt_batch_image_count.argtypes = [vp]
+    L.grt_batch_image_count.restype = C.c_size_t
+    L.grt_get_batch_image_products.argtypes = [vp, C.c_size_t, P(ImageProducts)]
+    L.grt_write_batch_products_npz.argtypes = [vp, C.c_char_p, C.c_char_p]
+    L.grt_render_graph.argtypes = [vp, P(RunStats)]
+    for name in ("grt_init_image_batch", "grt_get_batch_image_products", "grt_write_batch_products_npz",
+                 "grt_render_graph", "grt_trace_device_noalloc", "grt_measure_fma_peaks", "grt_params_validate", "grt_params_from_toml", "grt_create", "grt_set_params",
                  "grt_set_stream", "grt_synchronize", "grt_upload_grid", "grt_upload_grid_numpy_dir",
                  "grt_upload_photons", "grt_init_image_photons", "grt_run", "grt_download_photons",
                  "grt_get_image_products", "grt_write_image_products_npz", "grt_get_launch_config",
@@ -145,6 +152,7 @@ class Context:
         self.lib = load()
         self._h = C.c_void_p()
         self.params = params.copy()
+        self._specs = []
         rc = self.lib.grt_create(C.byref(self.params), C.byref(self._h))
         if rc != GRT_OK:
             raise GrtError(rc, "grt_create failed (needs an sm_100 device and valid params)")
@@ -203,6 +211,35 @@ class Context:
 
     def init_image_photons(self, nx, ny, id_offset=0):
         self._check(self.lib.grt_init_image_photons(self._h, nx, ny, id_offset))
+
+    def init_image_batch(self, specs, id_offset=0):
+        """Rays of several images (list of ImageSpec) for one batched launch."""
+        arr = (ImageSpec * len(specs))(*specs)
+        self._check(self.lib.grt_init_image_batch(self._h, arr, len(specs), id_offset))
+        self._specs = list(specs)
+
+    @property
+    def batch_image_count(self) -> int:
+        return int(self.lib.grt_batch_image_count(self._h))
+
+    def batch_image_products(self, image: int, out: ProductArrays | None = None) -> ProductArrays:
+        if out is None:
+            # an index the library will reject still gets valid buffers to pass
+            nx, ny = (self._specs[image].nx, self._specs[image].ny) if 0 <= image < len(self._specs) else (1, 1)
+            out = ProductArrays(nx, ny, self.params.spectrum_bins)
+        s = out.struct()
+        self._check(self.lib.grt_get_batch_image_products(self._h, image, C.byref(s)))
+        return out
+
+    def write_batch_products_npz(self, output_dir, name):
+        self._check(self.lib.grt_write_batch_products_npz(self._h, str(output_dir).encode(), name.encode()))
+
+    def render_graph(self) -> dict:
+        """Re-initialise, trace and build products through the context's CUDA graph."""
+        st = RunStats()
+        rc = self.lib.grt_render_graph(self._h, C.byref(st))
+        self._check(rc)
+        return st.as_dict()
 
     def run(self) -> dict:
         st = RunStats()

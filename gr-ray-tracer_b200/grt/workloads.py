@@ -22,7 +22,7 @@ from __future__ import annotations
 import math
 from dataclasses import dataclass, field
 
-from .abi import GEN_CUSTOM, MODE_IMAGE, PREC_FP64, RK4, RK45, Params
+from .abi import GEN_CUSTOM, MODE_IMAGE, PREC_FP64, RK4, RK45, ImageSpec, Params
 from .config import reference_defaults
 
 
@@ -72,7 +72,56 @@ C1 = ImageWorkload("c1_rk4_64px", (64, 32, 32), 0.9, 60.0, 64, RK4, 0.002, 1200)
 # RK45 rtol = atol = 1e-8, 256x256 px, 128x64x64 grid, a = 0.94, 17 deg.
 C2 = ImageWorkload("c2_rk45_256px", (128, 64, 64), 0.94, 17.0, 256, RK45, 0.01, 4000)
 
+# Frequency channels of a batch: custom generator frequency f and an emission
+# coefficient scaled by f / 230 GHz.
+FREQ_CHANNELS_GHZ = (230.0, 345.0, 86.0, 43.0)
+
+
+@dataclass
+class BatchWorkload:
+    """Several images traced by one persistent launch (grt_init_image_batch):
+    each entry is (inclination_deg, pixels, frequency_ghz)."""
+    name: str
+    base: ImageWorkload
+    images: list
+
+    def params(self) -> Params:
+        return self.base.params()
+
+    def specs(self, p: Params | None = None) -> list:
+        p = p or self.params()
+        out = []
+        for incl, px, f_ghz in self.images:
+            out.append(ImageSpec.from_params(p, px, px, camera_theta=math.radians(incl),
+                                             custom_frequency_hz=f_ghz * 1e9,
+                                             emission_coefficient=p.emission_coefficient * f_ghz / 230.0))
+        return out
+
+    @property
+    def rays(self) -> int:
+        return sum(px * px for _, px, _ in self.images)
+
+    def torus(self):
+        return self.base.torus()
+
+
+def _c3_images(seed=3):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    incl = np.linspace(5.0, 85.0, 16)
+    sizes = (64, 128, 256, 512)
+    return [(float(i), int(sizes[rng.integers(0, 4)]), f) for i in incl for f in FREQ_CHANNELS_GHZ]
+
+
+# The 256x256 RK45 image of C2 at the four frequency channels, one launch.
+C2_BATCH = BatchWorkload("c2_rk45_256px_x4freq", C2, [(C2.inclination_deg, C2.pixels, f) for f in FREQ_CHANNELS_GHZ])
+# 16 inclinations (5..85 deg) x 4 frequency channels, image sizes drawn from
+# {64,128,256,512}^2 (seeded), RK45 over a 128x64x64 torus with a = 0.9.
+C3 = BatchWorkload("c3_batch_64img", ImageWorkload("c3_base", (128, 64, 64), 0.9, 60.0, 256, RK45, 0.01, 4000),
+                   _c3_images())
+
 WORKLOADS = {"c1": C1, "c2": C2}
+BATCHES = {"c2": C2_BATCH, "c3": C3}
 
 
 def scaled(w: ImageWorkload, pixels=None, grid=None, **extra) -> ImageWorkload:

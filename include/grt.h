@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define GRT_ABI_VERSION 1
+#define GRT_ABI_VERSION 2
 
 typedef enum grt_status {
     GRT_OK = 0,
@@ -213,7 +213,12 @@ grt_status grt_upload_grid(grt_ctx* ctx, size_t nr, size_t ntheta, size_t nphi,
 /* Load the seven .npy files of a reference input directory and upload them. */
 grt_status grt_upload_grid_numpy_dir(grt_ctx* ctx, const char* numpy_dir);
 
-/* Copy n photons from host SoA into the context (replaces the Photons views). */
+/*
+ * Copy n photons from host SoA into the context (replaces the Photons views).
+ * After an image initialisation with the same photon count the slots keep
+ * their images (a saved batch state can be restored); otherwise the image set
+ * is dropped and every photon uses the camera of grt_params.
+ */
 grt_status grt_upload_photons(grt_ctx* ctx, const grt_photon_soa* soa, size_t n);
 
 /*
@@ -246,6 +251,54 @@ grt_status grt_get_image_products(grt_ctx* ctx, grt_image_products* out);
 
 /* Write <output_dir>/<name>_image_products.npz like write_image_products. */
 grt_status grt_write_image_products_npz(grt_ctx* ctx, const char* output_dir, const char* name);
+
+/*
+ * Batched image mode (no counterpart in the reference, which renders one
+ * camera per run): several images, each with its own camera and radiative
+ * coefficients (inclinations, resolutions, frequency channels), traced by ONE
+ * persistent launch whose work queue spans every image's rays, so long and
+ * short rays of all images balance across the GPU.  Each image follows
+ * grt_init_image_photons for its own camera; the other parameters come from
+ * the context's grt_params.
+ */
+typedef struct grt_image_spec {
+    double camera_theta;            /* camera.theta / camera.phi / distance / width / height of this image */
+    double camera_phi;
+    double camera_distance;
+    double camera_width;
+    double camera_height;
+    uint64_t nx, ny;                /* pixels = rays of this image */
+    double custom_frequency_hz;     /* photon_generation.custom_frequency_hz (custom generator) */
+    double absorption_coefficient;  /* radiative_transfer.absorption_coefficient */
+    double emission_coefficient;    /* radiative_transfer.emission_coefficient */
+} grt_image_spec;
+
+/*
+ * Initialise the rays of nimages images on the device: image k occupies the
+ * photon slots [start_k, start_k + nx_k*ny_k) with start_0 = 0 and ids
+ * id_offset + start_k + iy*nx_k + ix.  Replaces any earlier photons.
+ */
+grt_status grt_init_image_batch(grt_ctx* ctx, const grt_image_spec* specs, size_t nimages, uint64_t id_offset);
+size_t grt_batch_image_count(const grt_ctx* ctx);
+
+/* Products of image k of the batch (buffers sized nx_k*ny_k and p.spectrum_bins). */
+grt_status grt_get_batch_image_products(grt_ctx* ctx, size_t image, grt_image_products* out);
+
+/* Write <output_dir>/<name>_image<k>_image_products.npz for every image k. */
+grt_status grt_write_batch_products_npz(grt_ctx* ctx, const char* output_dir, const char* name);
+
+/*
+ * Render through a CUDA graph: re-initialise the rays of the last
+ * grt_init_image_photons / grt_init_image_batch call, trace them and build
+ * every image's products on the device.  The graph is captured on the first
+ * call and replayed afterwards (re-captured after a change of parameters,
+ * grid, images, stream or launch shape).  Needs termination_percent >= 1 (one
+ * trace launch, no host decision inside the loop), else GRT_EINVAL.
+ * stats->trace_ms is the trace kernel's time (event-record nodes inside the
+ * graph).  Products are then read with grt_get_image_products /
+ * grt_get_batch_image_products.
+ */
+grt_status grt_render_graph(grt_ctx* ctx, grt_run_stats* stats);
 
 /* Launch shape of the trace kernel. */
 grt_status grt_get_launch_config(const grt_ctx* ctx, grt_launch_config* cfg);

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_function():
     assert len(names) >= 20
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
-    assert L.grt_abi_version() == 1
+    assert L.grt_abi_version() == 2
 
 
 def test_struct_layout_matches_c(tmp_path):
@@ -35,7 +35,8 @@ def test_struct_layout_matches_c(tmp_path):
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "grt.h"', 'int main(void){']
     for cname, pyname in (("grt_params", abi.Params), ("grt_photon_soa", abi.PhotonSoA),
                           ("grt_run_stats", abi.RunStats), ("grt_image_products", abi.ImageProducts),
-                          ("grt_launch_config", abi.LaunchConfig), ("grt_device_grid", abi.DeviceGrid)):
+                          ("grt_launch_config", abi.LaunchConfig), ("grt_device_grid", abi.DeviceGrid),
+                          ("grt_image_spec", abi.ImageSpec)):
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
         for f, _ in pyname._fields_:
             lines.append(f'printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
@@ -46,7 +47,8 @@ def test_struct_layout_matches_c(tmp_path):
     out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split("\n") if line)
     for cname, pyname in (("grt_params", abi.Params), ("grt_photon_soa", abi.PhotonSoA),
                           ("grt_run_stats", abi.RunStats), ("grt_image_products", abi.ImageProducts),
-                          ("grt_launch_config", abi.LaunchConfig), ("grt_device_grid", abi.DeviceGrid)):
+                          ("grt_launch_config", abi.LaunchConfig), ("grt_device_grid", abi.DeviceGrid),
+                          ("grt_image_spec", abi.ImageSpec)):
         assert int(out[cname]) == C.sizeof(pyname), cname
         for f, _ in pyname._fields_:
             assert int(out[f"{cname}.{f}"]) == getattr(pyname, f).offset, f"{cname}.{f}"

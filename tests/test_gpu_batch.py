@@ -1,0 +1,175 @@
+"""Batched images (grt_init_image_batch) and the render graph (grt_render_graph).
+
+Every image of a batch runs the same per-ray arithmetic as that image traced
+alone (its camera, frequency and coefficients come from the image table, ids
+continue across images), so each image's photons and products must equal the
+single-image run bit for bit, and the single-image run is the oracle's."""
+
+import math
+
+import numpy as np
+import pytest
+
+from grt import abi, workloads
+from helpers import assert_photons_match, assert_products_match, mini, run_oracle, stokes_l2_rel
+
+pytestmark = pytest.mark.gpu
+
+SMALL = mini(workloads.C2, 16, (32, 16, 16))
+
+
+def batch_specs(p):
+    return [
+        abi.ImageSpec.from_params(p, 16, 16, camera_theta=math.radians(17.0)),
+        abi.ImageSpec.from_params(p, 12, 20, camera_theta=math.radians(60.0), custom_frequency_hz=86e9,
+                                  emission_coefficient=86.0 / 230.0),
+        abi.ImageSpec.from_params(p, 24, 24, camera_theta=math.radians(85.0), camera_phi=0.7,
+                                  custom_frequency_hz=345e9, emission_coefficient=1.5, absorption_coefficient=0.5),
+    ]
+
+
+def single_params(p, sp):
+    q = p.copy()
+    q.update(camera_theta=sp.camera_theta, camera_phi=sp.camera_phi, camera_distance=sp.camera_distance,
+             camera_width=sp.camera_width, camera_height=sp.camera_height, image_nx=sp.nx, image_ny=sp.ny,
+             custom_frequency_hz=sp.custom_frequency_hz, absorption_coefficient=sp.absorption_coefficient,
+             emission_coefficient=sp.emission_coefficient, nphotons=sp.nx * sp.ny)
+    return q
+
+
+def run_batch(lib, p, grid, specs, graph=False):
+    ctx = lib.Context(p)
+    try:
+        ctx.upload_grid(grid)
+        ctx.init_image_batch(specs)
+        assert ctx.batch_image_count == len(specs)
+        stats = ctx.render_graph() if graph else ctx.run()
+        ph = ctx.download_photons()
+        prods = [ctx.batch_image_products(k) for k in range(len(specs))]
+    finally:
+        ctx.close()
+    return ph, prods, stats
+
+
+def test_batch_equals_single_images(gpu, oracle):
+    p = SMALL.params()
+    grid = SMALL.torus()
+    specs = batch_specs(p)
+    ph, prods, stats = run_batch(gpu, p, grid, specs)
+    start = 0
+    accepted = 0
+    for k, sp in enumerate(specs):
+        q = single_params(p, sp)
+        n = sp.nx * sp.ny
+        ctx = gpu.Context(q)
+        try:
+            ctx.upload_grid(grid)
+            ctx.init_image_photons(sp.nx, sp.ny, id_offset=start)
+            st = ctx.run()
+            single = ctx.download_photons()
+            sprod = ctx.image_products()
+        finally:
+            ctx.close()
+        accepted += st["accepted_steps"]
+        for f in abi.PHOTON_FIELDS:
+            assert np.array_equal(getattr(ph, f)[start:start + n], getattr(single, f)), (k, f)
+        for f in ("image_I", "image_Q", "image_U", "image_V", "spectrum_frequency_hz", "arrived_count"):
+            assert np.array_equal(getattr(prods[k], f), getattr(sprod, f)), (k, f)
+        # spectrum bins sum many photons with atomics: equal up to summation order
+        assert_products_match(prods[k], sprod)
+        # and the single image is the oracle's
+        init = oracle.init_image_photons(q, sp.nx, sp.ny, id_offset=start)
+        want, wprod, _ = run_oracle(oracle, q, grid, photons=init)
+        assert_photons_match(single, want)
+        assert_products_match(sprod, wprod)
+        start += n
+    assert stats["accepted_steps"] == accepted
+    assert stats["n_terminated"] == start
+
+
+def test_render_graph_matches_run(gpu):
+    p = SMALL.params()
+    grid = SMALL.torus()
+    specs = batch_specs(p)
+    ph, prods, st = run_batch(gpu, p, grid, specs)
+    ctx = gpu.Context(p)
+    try:
+        ctx.upload_grid(grid)
+        ctx.init_image_batch(specs)
+        for _ in range(3):  # capture, then replays from the re-initialised rays
+            gst = ctx.render_graph()
+            assert gst["accepted_steps"] == st["accepted_steps"]
+            assert gst["steps_done"] == st["steps_done"]
+            gph = ctx.download_photons()
+            for f in abi.PHOTON_FIELDS:
+                assert np.array_equal(getattr(gph, f), getattr(ph, f)), f
+            for k in range(len(specs)):
+                assert np.array_equal(ctx.batch_image_products(k).image_I, prods[k].image_I)
+        # a parameter change re-captures
+        q = p.copy()
+        q.emission_coefficient = 2.0
+        ctx.set_params(q)
+        ctx.init_image_batch(specs)
+        ctx.render_graph()
+        assert not np.array_equal(ctx.batch_image_products(0).image_I, prods[0].image_I) or \
+            not prods[0].image_I.any()
+    finally:
+        ctx.close()
+
+
+def test_render_graph_single_image(gpu):
+    w = SMALL
+    p = w.params()
+    grid = w.torus()
+    ctx = gpu.Context(p)
+    try:
+        ctx.upload_grid(grid)
+        ctx.init_image_photons(w.pixels, w.pixels)
+        st = ctx.run()
+        want = ctx.image_products()
+        ctx.init_image_photons(w.pixels, w.pixels)
+        gst = ctx.render_graph()
+        got = ctx.image_products()
+        assert gst["accepted_steps"] == st["accepted_steps"]
+        assert np.array_equal(got.image_I, want.image_I)
+        # chunked runs cannot be captured
+        q = p.copy()
+        q.termination_percent = 0.5
+        ctx.set_params(q)
+        with pytest.raises(gpu.GrtError):
+            ctx.render_graph()
+    finally:
+        ctx.close()
+
+
+def test_batch_rejects_bad_specs(gpu):
+    p = SMALL.params()
+    ctx = gpu.Context(p)
+    try:
+        with pytest.raises(gpu.GrtError):
+            ctx.init_image_batch([abi.ImageSpec.from_params(p, 0, 16)])
+        with pytest.raises(gpu.GrtError):
+            ctx.init_image_batch([abi.ImageSpec.from_params(p, 16, 16, camera_width=0.0)])
+        with pytest.raises(gpu.GrtError):
+            ctx.batch_image_products(0)
+    finally:
+        ctx.close()
+
+
+def test_mixed_precision_batch_error(gpu):
+    # each frequency channel of the C2 image (at 64x64 on a 64x32x32 grid) in
+    # the mixed form against the FP64 form: L2 relative Stokes-I error <= 1e-5
+    base = mini(workloads.C2, 64, (64, 32, 32))
+    bw = workloads.BatchWorkload("c2_small_x4freq", base,
+                                 [(base.inclination_deg, base.pixels, f) for f in workloads.FREQ_CHANNELS_GHZ])
+    p = bw.params()
+    grid = bw.torus()
+    specs = bw.specs(p)
+    _, ref, _ = run_batch(gpu, p, grid, specs)
+    pm = p.copy()
+    pm.precision = abi.PREC_MIXED
+    _, got, _ = run_batch(gpu, pm, grid, specs)
+    for k in range(len(specs)):
+        assert ref[k].image_I.any()
+        err = stokes_l2_rel(got[k].image_I, ref[k].image_I)
+        assert err <= 1e-5, (k, err)
