@@ -123,6 +123,7 @@ struct grt_ctx {
     std::vector<grt_image_spec> images;
     std::vector<unsigned long long> image_start;
     uint64_t image_id_offset = 0;
+    double forward_back = 0.0;  // > 0: line-of-sight forward rays from -forward_back * n
     bool batched = false;      // trace kernels read the per-image table
     bool have_images = false;  // photons came from an image init (a render can re-initialise them)
     DevBuf<grt::KImage> images_dev;
@@ -132,6 +133,15 @@ struct grt_ctx {
     DevBuf<unsigned long long> barrived;
     std::vector<size_t> bimage_off;
     bool bproducts_valid = false;
+    // per-cell multipliers on dtau / dI (differentiable RT)
+    DevBuf<double> m_abs, m_emis;
+    bool has_m_abs = false, has_m_emis = false;
+    // checkpointed forward / adjoint
+    DevBuf<double> ckpt, tape, dLdI, g_abs, g_emis;
+    DevBuf<int> nckpt, adj_overflow;
+    DevBuf<long long> call0;
+    int adj_K = 0, adj_cap = 0;
+    bool adj_ready = false;
     // render graph, valid while generation == graph_generation
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -271,6 +281,8 @@ grt::KParams make_kparams(const grt_ctx* c) {
     g.mag = c->mag.ptr;
     g.r_reject_lo = c->r_reject_lo;
     g.r_reject_hi = c->r_reject_hi;
+    k.m_abs = c->has_m_abs ? c->m_abs.ptr : nullptr;
+    k.m_emis = c->has_m_emis ? c->m_emis.ptr : nullptr;
     if (c->batched) {
         k.images = c->images_dev.ptr;
         k.image_start = c->image_start_dev.ptr;
@@ -340,6 +352,9 @@ void grt_destroy(grt_ctx* c) {
     c->counters.release();
     c->image.release(); c->spectrum.release(); c->arrived.release(); c->scratch_u64.release();
     c->images_dev.release(); c->image_start_dev.release();
+    c->m_abs.release(); c->m_emis.release();
+    c->ckpt.release(); c->tape.release(); c->dLdI.release(); c->g_abs.release(); c->g_emis.release();
+    c->nckpt.release(); c->adj_overflow.release(); c->call0.release();
     c->bimage.release(); c->bspectrum.release(); c->barrived.release();
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
@@ -528,6 +543,7 @@ grt_status grt_upload_photons(grt_ctx* c, const grt_photon_soa* s, size_t n) {
     if (!c || (!s && n)) return GRT_EINVAL;
     if (n > (1ull << 40)) return fail(c, GRT_EINVAL, "photon count too large");
     const bool keep_images = c->have_images && n == c->n;  // same slots: photons keep their images
+    c->adj_ready = false;
     GRT_CUDA(c, c->ph.alloc(n), "alloc photons");
     c->n = n;
     c->bproducts_valid = false;
@@ -618,12 +634,22 @@ grt_status launch_image_inits(grt_ctx* c) {
         a.a = p.spin;
         a.M = p.mass;
         a.dlambda0 = p.initial_step * sp.camera_distance;
+        a.forward = c->forward_back > 0.0;
+        if (a.forward) {
+            const double B = c->forward_back;
+            a.bx = -B * std::sin(sp.camera_theta) * std::cos(sp.camera_phi);
+            a.by = -B * std::sin(sp.camera_theta) * std::sin(sp.camera_phi);
+            a.bz = -B * std::cos(sp.camera_theta);
+            a.dlambda0 = p.initial_step * B;
+            a.nu0 = sp.custom_frequency_hz;
+        }
         GRT_CUDA(c, grt::launch_init_image(a, c->stream), "init_image_pixels");
     }
     return GRT_OK;
 }
 
-grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages, uint64_t id_offset, bool batched) {
+grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages, uint64_t id_offset, bool batched,
+                         double forward_back = 0.0) {
     unsigned long long total = 0;
     std::vector<unsigned long long> start(nimages + 1, 0);
     for (size_t k = 0; k < nimages; ++k) {
@@ -646,9 +672,11 @@ grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages
     c->images.assign(specs, specs + nimages);
     c->image_start = start;
     c->image_id_offset = id_offset;
+    c->forward_back = forward_back;
     c->batched = batched;
     c->have_images = true;
     c->bproducts_valid = false;
+    c->adj_ready = false;
     if (batched) {
         const grt_params& p = c->p;
         std::vector<grt::KImage> tab(nimages);
@@ -778,6 +806,16 @@ grt_status grt_init_image_photons(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t
     return set_image_set(c, &sp, 1, id_offset, false);
 }
 
+grt_status grt_init_image_forward_photons(grt_ctx* c, uint64_t nx, uint64_t ny, double back_distance,
+                                          uint64_t id_offset) {
+    if (!c) return GRT_EINVAL;
+    if (!(back_distance > 0.0) || !std::isfinite(back_distance))
+        return fail(c, GRT_EINVAL, "back_distance must be positive");
+    if (nx * ny == 0) return fail(c, GRT_EINVAL, "nx and ny must be positive");
+    const grt_image_spec sp = spec_from_params(c->p, nx, ny);
+    return set_image_set(c, &sp, 1, id_offset, false, back_distance);
+}
+
 grt_status grt_init_image_batch(grt_ctx* c, const grt_image_spec* specs, size_t nimages, uint64_t id_offset) {
     if (!c) return GRT_EINVAL;
     if (!specs || nimages == 0) return fail(c, GRT_EINVAL, "an image batch needs at least one image");
@@ -822,6 +860,7 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
     grt_run_stats st;
     std::memset(&st, 0, sizeof(st));
     c->bproducts_valid = false;
+    c->adj_ready = false;
     if (c->n == 0) {
         st.steps_done = p.max_steps;
         if (stats) *stats = st;
@@ -949,6 +988,7 @@ grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
     GRT_CUDA(c, cudaStreamSynchronize(c->stream), "render graph");
     c->initial_terminated = 0;
     c->bproducts_valid = true;
+    c->adj_ready = false;
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     const grt::KCounters& k = *c->host_counters;
@@ -967,6 +1007,150 @@ grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
         return fail(c, GRT_ETIMEOUT, "trace kernel hit its iteration limit");
     }
     if (stats) *stats = st;
+    return GRT_OK;
+}
+
+grt_status grt_set_cell_multipliers(grt_ctx* c, const double* m_abs, const double* m_emis) {
+    if (!c) return GRT_EINVAL;
+    const size_t ncell = static_cast<size_t>(c->nr) * c->nth * c->nph;
+    if ((m_abs || m_emis) && (!c->grid_uploaded || !c->fluid_available || ncell == 0))
+        return fail(c, GRT_ESTATE, "cell multipliers need an uploaded fluid grid");
+    ++c->generation;
+    c->adj_ready = false;
+    c->has_m_abs = c->has_m_emis = false;
+    if (m_abs) {
+        GRT_CUDA(c, c->m_abs.alloc(ncell), "alloc multipliers");
+        GRT_CUDA(c, cudaMemcpy(c->m_abs.ptr, m_abs, ncell * sizeof(double), cudaMemcpyHostToDevice), "H2D");
+        c->has_m_abs = true;
+    }
+    if (m_emis) {
+        GRT_CUDA(c, c->m_emis.alloc(ncell), "alloc multipliers");
+        GRT_CUDA(c, cudaMemcpy(c->m_emis.ptr, m_emis, ncell * sizeof(double), cudaMemcpyHostToDevice), "H2D");
+        c->has_m_emis = true;
+    }
+    return GRT_OK;
+}
+
+grt_status grt_forward_checkpointed(grt_ctx* c, int64_t K, grt_run_stats* stats) {
+    if (!c) return GRT_EINVAL;
+    if (!c->grid_uploaded) return fail(c, GRT_ESTATE, "grt_forward_checkpointed before grt_upload_grid");
+    const grt_params& p = c->p;
+    if (K < 1 || K > (1 << 20)) return fail(c, GRT_EINVAL, "checkpoint_interval must be in [1, 2^20]");
+    if (!(p.termination_percent >= 1.0))
+        return fail(c, GRT_EINVAL, "the checkpointed forward needs termination_percent >= 1");
+    if (p.precision != GRT_PREC_FP64) return fail(c, GRT_EINVAL, "the checkpointed forward runs the FP64 form");
+    grt_run_stats st;
+    std::memset(&st, 0, sizeof(st));
+    c->adj_ready = false;
+    c->bproducts_valid = false;
+    const size_t n = c->n;
+    const long long cap = (p.max_steps + K - 1) / K + 1;
+    const double bytes = static_cast<double>(n) * static_cast<double>(cap) * 16.0 * 8.0;
+    if (bytes > 32.0 * (1ull << 30))
+        return fail(c, GRT_ENOMEM, "checkpoints would need " + std::to_string(bytes / (1ull << 30)) +
+                                       " GiB; raise checkpoint_interval");
+    const int threads = 128;
+    const long long want_blocks = (static_cast<long long>(n) + threads - 1) / threads;
+    const int blocks = static_cast<int>(std::max(1ll, std::min<long long>(want_blocks, 8ll * c->sm_count)));
+    GRT_CUDA(c, c->ckpt.alloc(n * cap * 16), "alloc checkpoints");
+    GRT_CUDA(c, c->nckpt.alloc(std::max<size_t>(n, 1)), "alloc checkpoints");
+    GRT_CUDA(c, c->call0.alloc(std::max<size_t>(n, 1)), "alloc checkpoints");
+    GRT_CUDA(c, c->adj_overflow.alloc(1), "alloc checkpoints");
+    GRT_CUDA(c, c->tape.alloc(static_cast<size_t>(blocks) * threads * K * 6), "alloc tape");
+    c->adj_K = static_cast<int>(K);
+    c->adj_cap = static_cast<int>(cap);
+    if (n == 0) {
+        st.steps_done = p.max_steps;
+        if (stats) *stats = st;
+        c->adj_ready = true;
+        return GRT_OK;
+    }
+    grt::KParams kp = make_kparams(c);
+    kp.step0 = 0;
+    kp.budget = p.max_steps;
+    grt::AdjointArgs aa{};
+    aa.ckpt = c->ckpt.ptr;
+    aa.cap = c->adj_cap;
+    aa.K = c->adj_K;
+    aa.nckpt = c->nckpt.ptr;
+    aa.call0 = c->call0.ptr;
+    aa.overflow = c->adj_overflow.ptr;
+    GRT_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, sizeof(grt::KCounters), c->stream), "memset");
+    GRT_CUDA(c, cudaMemsetAsync(c->adj_overflow.ptr, 0, sizeof(int), c->stream), "memset");
+    GRT_CUDA(c, cudaEventRecord(c->ev0, c->stream), "event");
+    cudaError_t e = grt::launch_adjoint_forward(kp, aa, blocks, trace_smem(c), c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "adjoint forward launch");
+    GRT_CUDA(c, cudaEventRecord(c->ev1, c->stream), "event");
+    GRT_CUDA(c, cudaMemcpyAsync(c->host_counters, c->counters.ptr, sizeof(grt::KCounters), cudaMemcpyDeviceToHost,
+                                c->stream), "D2H counters");
+    int overflow = 0;
+    GRT_CUDA(c, cudaMemcpyAsync(&overflow, c->adj_overflow.ptr, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+             "D2H");
+    GRT_CUDA(c, cudaStreamSynchronize(c->stream), "adjoint forward");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    if (overflow) return fail(c, GRT_ECUDA, "checkpoint capacity exceeded");
+    const grt::KCounters& k = *c->host_counters;
+    st.photon_calls = k.calls;
+    st.n_terminated = k.terminated + c->initial_terminated;
+    st.launches = 1;
+    st.trace_ms = ms;
+    st.steps_done = p.max_steps;
+    if (stats) *stats = st;
+    c->adj_ready = true;
+    return GRT_OK;
+}
+
+grt_status grt_adjoint_image_I(grt_ctx* c, const double* dL_dI, double* g_abs, double* g_emis) {
+    if (!c || !dL_dI) return GRT_EINVAL;
+    if (!c->adj_ready) return fail(c, GRT_ESTATE, "grt_adjoint_image_I needs a grt_forward_checkpointed first");
+    if (c->batched) return fail(c, GRT_EINVAL, "the adjoint covers single-image runs");
+    const grt_params& p = c->p;
+    const size_t ncell = static_cast<size_t>(c->nr) * c->nth * c->nph;
+    const size_t npix = p.image_nx * p.image_ny;
+    GRT_CUDA(c, c->dLdI.alloc(std::max<size_t>(npix, 1)), "alloc");
+    GRT_CUDA(c, c->g_abs.alloc(std::max<size_t>(ncell, 1)), "alloc");
+    GRT_CUDA(c, c->g_emis.alloc(std::max<size_t>(ncell, 1)), "alloc");
+    GRT_CUDA(c, cudaMemcpyAsync(c->dLdI.ptr, dL_dI, npix * sizeof(double), cudaMemcpyHostToDevice, c->stream), "H2D");
+    GRT_CUDA(c, cudaMemsetAsync(c->g_abs.ptr, 0, std::max<size_t>(ncell, 1) * sizeof(double), c->stream), "memset");
+    GRT_CUDA(c, cudaMemsetAsync(c->g_emis.ptr, 0, std::max<size_t>(ncell, 1) * sizeof(double), c->stream), "memset");
+    GRT_CUDA(c, cudaMemsetAsync(c->adj_overflow.ptr, 0, sizeof(int), c->stream), "memset");
+    if (c->n > 0 && ncell > 0) {
+        grt::KParams kp = make_kparams(c);
+        kp.step0 = 0;
+        kp.budget = p.max_steps;
+        grt::AdjointArgs aa{};
+        aa.ckpt = c->ckpt.ptr;
+        aa.cap = c->adj_cap;
+        aa.K = c->adj_K;
+        aa.nckpt = c->nckpt.ptr;
+        aa.call0 = c->call0.ptr;
+        aa.overflow = c->adj_overflow.ptr;
+        aa.dL_dI = c->dLdI.ptr;
+        aa.nx = p.image_nx;
+        aa.ny = p.image_ny;
+        aa.W = p.camera_width;
+        aa.H = p.camera_height;
+        aa.g_abs = c->g_abs.ptr;
+        aa.g_emis = c->g_emis.ptr;
+        aa.tape = c->tape.ptr;
+        const int threads = 128;
+        const size_t tape_threads = c->tape.count / (static_cast<size_t>(c->adj_K) * 6);
+        const int blocks = static_cast<int>(std::max<size_t>(1, tape_threads / threads));
+        cudaError_t e = grt::launch_adjoint_reverse(kp, aa, blocks, trace_smem(c), c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "adjoint reverse launch");
+    }
+    int overflow = 0;
+    GRT_CUDA(c, cudaMemcpyAsync(&overflow, c->adj_overflow.ptr, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+             "D2H");
+    if (g_abs && ncell)
+        GRT_CUDA(c, cudaMemcpyAsync(g_abs, c->g_abs.ptr, ncell * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                 "D2H gradient");
+    if (g_emis && ncell)
+        GRT_CUDA(c, cudaMemcpyAsync(g_emis, c->g_emis.ptr, ncell * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                 "D2H gradient");
+    GRT_CUDA(c, cudaStreamSynchronize(c->stream), "adjoint reverse");
+    if (overflow) return fail(c, GRT_ECUDA, "adjoint tape capacity exceeded");
     return GRT_OK;
 }
 

@@ -23,16 +23,18 @@ __global__ void __launch_bounds__(128, MINB) trace_fp64(const __grid_constant__ 
 
 // initialize_photons.hpp:116-169 with screen (u, v) at pixel centres; the
 // camera centre and basis come from the host (glibc sin/cos, like the reference).
+// With args.forward, line-of-sight forward rays instead (see InitImageArgs).
 __global__ void init_image_pixels(const __grid_constant__ InitImageArgs args) {
     const unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
     if (i >= args.nx * args.ny) return;
     const unsigned long long iy = i / args.nx, ix = i % args.nx;
     const double u = -0.5 * args.W + (static_cast<double>(ix) + 0.5) * args.W / static_cast<double>(args.nx);
     const double v = -0.5 * args.H + (static_cast<double>(iy) + 0.5) * args.H / static_cast<double>(args.ny);
-    const double x = args.cx + u * args.th_hat[0] + v * args.ph_hat[0];
-    const double y = args.cy + u * args.th_hat[1] + v * args.ph_hat[1];
-    const double z = args.cz + u * args.th_hat[2] + v * args.ph_hat[2];
-    double kx = -args.cx, ky = -args.cy, kz = -args.cz;
+    const bool fwd = args.forward != 0;
+    const double x = (fwd ? args.bx : args.cx) + u * args.th_hat[0] + v * args.ph_hat[0];
+    const double y = (fwd ? args.by : args.cy) + u * args.th_hat[1] + v * args.ph_hat[1];
+    const double z = (fwd ? args.bz : args.cz) + u * args.th_hat[2] + v * args.ph_hat[2];
+    double kx = fwd ? args.cx : -args.cx, ky = fwd ? args.cy : -args.cy, kz = fwd ? args.cz : -args.cz;
     const double kn = sqrt(kx * kx + ky * ky + kz * kz);
     kx /= kn;
     ky /= kn;
@@ -44,26 +46,18 @@ __global__ void init_image_pixels(const __grid_constant__ InitImageArgs args) {
     const KPhotons& P = args.ph;
     const unsigned long long o = args.offset + i;
     P.id[o] = args.id_offset + i;
-    P.frequency[o] = 0.0;
-    P.emission_frame_energy[o] = 1.0;
+    P.frequency[o] = fwd ? args.nu0 : 0.0;
+    P.emission_frame_energy[o] = fwd ? -p[0] : 1.0;
     P.x0[o] = 0.0; P.x1[o] = x; P.x2[o] = y; P.x3[o] = z;
     P.k0[o] = p[0]; P.k1[o] = p[1]; P.k2[o] = p[2]; P.k3[o] = p[3];
     P.I[o] = 0.0; P.Q[o] = 0.0; P.U[o] = 0.0; P.V[o] = 0.0;
     P.dlambda[o] = args.dlambda0;
     P.terminate[o] = 0;
-    P.phase[o] = 1;  // ImageBackward
+    P.phase[o] = fwd ? 2 : 1;  // ImageForward / ImageBackward
     P.theta_disp[o] = u;
     P.phi_disp[o] = v;
 }
 
-// observation.hpp:22-29
-__device__ __forceinline__ unsigned long long observation_bin(double value, double lo, double hi,
-                                                              unsigned long long bins) {
-    if (bins <= 1 || !(hi > lo)) return 0;
-    const double f = (value - lo) / (hi - lo);
-    const double sc = fmax(0.0, fmin(1.0, f));
-    return static_cast<unsigned long long>(sc * static_cast<double>(bins - 1));
-}
 
 // observation.hpp:61-82: ImageArrived photons binned by arrival (u, v) and log10(nu).
 __global__ void image_products(const __grid_constant__ ProductsArgs args) {
@@ -73,8 +67,8 @@ __global__ void image_products(const __grid_constant__ ProductsArgs args) {
         const unsigned long long o = args.offset + i;
         if (args.ph.phase[o] == 3) {
             arrived = true;
-            const unsigned long long px = observation_bin(args.ph.theta_disp[o], -0.5 * args.W, 0.5 * args.W, args.nx);
-            const unsigned long long py = observation_bin(args.ph.phi_disp[o], -0.5 * args.H, 0.5 * args.H, args.ny);
+            const unsigned long long px = dev::observation_bin(args.ph.theta_disp[o], -0.5 * args.W, 0.5 * args.W, args.nx);
+            const unsigned long long py = dev::observation_bin(args.ph.phi_disp[o], -0.5 * args.H, 0.5 * args.H, args.ny);
             const unsigned long long pix = py * args.nx + px;
             const double I = args.ph.I[o];
             atomicAdd(&args.image[pix], I);
@@ -83,7 +77,7 @@ __global__ void image_products(const __grid_constant__ ProductsArgs args) {
             atomicAdd(&args.image[3 * args.nx * args.ny + pix], args.ph.V[o]);
             const double f = args.ph.frequency[o];
             if (f >= args.spec_min && f <= args.spec_max) {
-                const unsigned long long b = observation_bin(log10(f), args.log_min, args.log_max, args.bins);
+                const unsigned long long b = dev::observation_bin(log10(f), args.log_min, args.log_max, args.bins);
                 atomicAdd(&args.spectrum[b], I);
             }
         }

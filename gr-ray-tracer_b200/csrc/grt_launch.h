@@ -20,7 +20,12 @@ struct InitImageArgs {
     double cx, cy, cz;
     double th_hat[3], ph_hat[3];
     double a, M;
-    double dlambda0;               // initial_step * camera_distance
+    double dlambda0;               // initial_step * camera_distance (forward: * back distance)
+    // line-of-sight forward rays: start on the plane -back * n, aimed along +n,
+    // ImageForward, I = 0, frequency nu0, emission_frame_energy = -p_t
+    int forward;
+    double bx, by, bz;             // -back * n
+    double nu0;
 };
 
 struct ProductsArgs {
@@ -32,6 +37,22 @@ struct ProductsArgs {
     double* image;                 // [4][ny][nx] (I, Q, U, V)
     double* spectrum;              // [bins]
     unsigned long long* arrived;   // [1]
+};
+
+// Buffers of the adjoint pass (grt_adjoint.cu).
+struct AdjointArgs {
+    double* ckpt;              // [n][cap][16] ray state after emission and every K calls
+    int cap;                   // checkpoints per ray
+    int K;                     // calls between checkpoints
+    int* nckpt;                // [n] checkpoints written
+    long long* call0;          // [n] calls taken when checkpoint 0 was written (-1: never emitted)
+    int* overflow;             // checkpoint/tape capacity errors
+    const double* dL_dI;       // [ny][nx] dL/d(image_I)
+    unsigned long long nx, ny;
+    double W, H;
+    double* g_abs;             // [ncell] dL/dm_abs (accumulated)
+    double* g_emis;            // [ncell] dL/dm_emis
+    double* tape;              // [threads][K][6]
 };
 
 // Camera plane basis of integrate_cart_ks.hpp:97-107 with host libm, plus the
@@ -64,6 +85,12 @@ inline size_t dev_trace_smem_bytes(int integrator, int threads, bool separable, 
     if (separable) n += 2 * static_cast<size_t>(nr + nth + nph);
     return n * sizeof(double);
 }
+
+// Adjoint pass: checkpointed forward trace and reverse sweep, 128-thread blocks.
+cudaError_t launch_adjoint_forward(const KParams& kp, const AdjointArgs& aa, int blocks, size_t smem,
+                                   cudaStream_t stream);
+cudaError_t launch_adjoint_reverse(const KParams& kp, const AdjointArgs& aa, int blocks, size_t smem,
+                                   cudaStream_t stream);
 
 // Persistent trace launches: sm_count * blocks_per_sm blocks of 128 threads;
 // blocks_per_sm in {2, 3, 4} picks the register cap (255 / 170 / 128).

@@ -256,9 +256,6 @@ struct LaneCounters {
     unsigned long long terminated, accepted, rejected, calls, max_term_step;
 };
 
-// Everything after the integration step of one call (integrate_cart_ks.hpp:307-417).
-// phase0 is the phase loaded at the start of the call.  Returns 1 if the photon
-// terminated.
 // The image a photon belongs to: the launch's only image, or the batch entry
 // whose index range holds photon index q (binary search, once per load).
 GRT_DEV int image_of_photon(const KParams& kp, long long q) {
@@ -274,9 +271,31 @@ GRT_DEV int image_of_photon(const KParams& kp, long long q) {
 
 GRT_DEV const KImage& image_params(const KParams& kp, int img) { return kp.nimages > 0 ? kp.images[img] : kp.img0; }
 
-template <bool RAW = false>
+// observation.hpp:22-29: bin of value in [lo, hi] over `bins` bins,
+// floor(clamp((value - lo) / (hi - lo)) * (bins - 1)).
+GRT_DEV unsigned long long observation_bin(double value, double lo, double hi, unsigned long long bins) {
+    if (bins <= 1 || !(hi > lo)) return 0;
+    const double f = (value - lo) / (hi - lo);
+    const double sc = fmax(0.0, fmin(1.0, f));
+    return static_cast<unsigned long long>(sc * static_cast<double>(bins - 1));
+}
+
+// Observer of the radiative-transfer updates of post_step (the adjoint's
+// recompute records them); the trace kernels pass NoRecord, which compiles away.
+struct NoRecord {
+    // one RT update in cell `cell`: I = (I_before * att + m_emis * j0) * scale,
+    // att = exp(-m_abs * tau0)
+    GRT_DEV void rt_step(int, double, double, double, double, double) {}
+    // the Stokes vector was zeroed (invalid arrival energies)
+    GRT_DEV void zeroed() {}
+};
+
+// Everything after the integration step of one call (integrate_cart_ks.hpp:307-417).
+// phase0 is the phase loaded at the start of the call.  Returns 1 if the photon
+// terminated.
+template <bool RAW = false, class Rec = NoRecord>
 GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, double taken, int64_t step,
-                      double& tdisp, double& pdisp, int& have_disp) {
+                      double& tdisp, double& pdisp, int& have_disp, Rec rec = Rec()) {
     const KImage& im = image_params(kp, L.img);
     L.radius = ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
     L.have_radius = 1;
@@ -314,15 +333,19 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
             terminated = 1;
         }
     } else if (sampled && !backward) {
+        const double I_before = L.I[0];
+        double tau0 = 0.0, j0 = 0.0, att = 1.0, scale = 1.0;
         if (kp.abs_on) {
             double dtau = ComputeOpticalDepthIncrement(fs.fluid, L.freq, taken, im.kappa);
+            tau0 = dtau;
             if (kp.m_abs) dtau = kp.m_abs[fs.cell] * dtau;
-            const double att = exp(-dtau);
+            att = exp(-dtau);
 #pragma unroll
             for (int q = 0; q < 4; ++q) L.I[q] *= att;
         }
         if (kp.emis_on) {
             double dI = ComputeEmissivityIncrement(fs.fluid, L.freq, taken, im.jcoef);
+            j0 = dI;
             if (kp.m_emis) dI = kp.m_emis[fs.cell] * dI;
             L.I[0] += dI;
         }
@@ -338,8 +361,10 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
                 for (int c = 4; c < 8; ++c) L.s[c] = st.s[c];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) L.I[q] = st.I[q];
+                scale = kp.albedo;
             }
         }
+        rec.rt_step(fs.cell, tau0, j0, I_before, att, scale);
     }
     if (kp.image_mode && phase0 == 2) {  // ImageForward
         double u = 0.0, v = 0.0;
@@ -351,6 +376,7 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
                 L.freq *= eo / ee;
             } else {
                 L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+                rec.zeroed();
             }
             tdisp = u;
             pdisp = v;

@@ -83,7 +83,13 @@ def load(path: Path | None = None):
     L.grt_get_batch_image_products.argtypes = [vp, C.c_size_t, P(ImageProducts)]
     L.grt_write_batch_products_npz.argtypes = [vp, C.c_char_p, C.c_char_p]
     L.grt_render_graph.argtypes = [vp, P(RunStats)]
-    for name in ("grt_init_image_batch", "grt_get_batch_image_products", "grt_write_batch_products_npz",
+    L.grt_init_image_forward_photons.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_double, C.c_uint64]
+    L.grt_init_image_forward_photons.restype = C.c_int
+    L.grt_set_cell_multipliers.argtypes = [vp, P(C.c_double), P(C.c_double)]
+    L.grt_forward_checkpointed.argtypes = [vp, C.c_int64, P(RunStats)]
+    L.grt_adjoint_image_I.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_double)]
+    for name in ("grt_set_cell_multipliers", "grt_forward_checkpointed", "grt_adjoint_image_I",
+                 "grt_init_image_batch", "grt_get_batch_image_products", "grt_write_batch_products_npz",
                  "grt_render_graph", "grt_trace_device_noalloc", "grt_measure_fma_peaks", "grt_params_validate", "grt_params_from_toml", "grt_create", "grt_set_params",
                  "grt_set_stream", "grt_synchronize", "grt_upload_grid", "grt_upload_grid_numpy_dir",
                  "grt_upload_photons", "grt_init_image_photons", "grt_run", "grt_download_photons",
@@ -212,6 +218,10 @@ class Context:
     def init_image_photons(self, nx, ny, id_offset=0):
         self._check(self.lib.grt_init_image_photons(self._h, nx, ny, id_offset))
 
+    def init_image_forward_photons(self, nx, ny, back_distance, id_offset=0):
+        """Line-of-sight forward rays behind the scene, aimed at the camera."""
+        self._check(self.lib.grt_init_image_forward_photons(self._h, nx, ny, float(back_distance), id_offset))
+
     def init_image_batch(self, specs, id_offset=0):
         """Rays of several images (list of ImageSpec) for one batched launch."""
         arr = (ImageSpec * len(specs))(*specs)
@@ -240,6 +250,29 @@ class Context:
         rc = self.lib.grt_render_graph(self._h, C.byref(st))
         self._check(rc)
         return st.as_dict()
+
+    # ---- differentiable radiative transfer ----
+    def set_cell_multipliers(self, m_abs=None, m_emis=None):
+        """Per-cell multipliers on dtau and dI (arrays of the grid's shape; None = 1)."""
+        self._mult = [None if m is None else np.ascontiguousarray(m, dtype=np.float64).ravel()
+                      for m in (m_abs, m_emis)]
+        self._check(self.lib.grt_set_cell_multipliers(self._h, *[_dp(m) if m is not None else None
+                                                                  for m in self._mult]))
+
+    def forward_checkpointed(self, checkpoint_interval: int = 64) -> dict:
+        st = RunStats()
+        self._check(self.lib.grt_forward_checkpointed(self._h, int(checkpoint_interval), C.byref(st)))
+        return st.as_dict()
+
+    def adjoint_image_I(self, dL_dimage_I, grid_shape):
+        """(dL/dm_abs, dL/dm_emis) of the last forward_checkpointed, each of grid_shape."""
+        g = np.ascontiguousarray(dL_dimage_I, dtype=np.float64)
+        if g.shape != (self.params.image_ny, self.params.image_nx):
+            raise ValueError(f"dL/dimage_I must have shape {(self.params.image_ny, self.params.image_nx)}")
+        ga = np.zeros(int(np.prod(grid_shape)))
+        ge = np.zeros(int(np.prod(grid_shape)))
+        self._check(self.lib.grt_adjoint_image_I(self._h, _dp(g), _dp(ga), _dp(ge)))
+        return ga.reshape(grid_shape), ge.reshape(grid_shape)
 
     def run(self) -> dict:
         st = RunStats()

@@ -120,6 +120,27 @@ C2_BATCH = BatchWorkload("c2_rk45_256px_x4freq", C2, [(C2.inclination_deg, C2.pi
 C3 = BatchWorkload("c3_batch_64img", ImageWorkload("c3_base", (128, 64, 64), 0.9, 60.0, 256, RK45, 0.01, 4000),
                    _c3_images())
 
+# Adjoint: 128x128 Stokes-I image, 96x48x48 torus, a = 0.9, 60 deg, RK45,
+# checkpoints every 64 calls.  The image is made of line-of-sight forward rays
+# (grt_init_image_forward_photons): the reference's own image mode emits at
+# the first fluid contact and retraces its path outward, so its forward leg
+# samples no fluid and the image does not depend on the multipliers at all.
+# Forward rays start C4_BACK_DISTANCE behind the scene, cross the torus and
+# are binned where they cross the camera plane, here at 100 M with a +/-30 M
+# window so that lensed rays still land on it.
+C4 = ImageWorkload("c4_adjoint_128px", (96, 48, 48), 0.9, 60.0, 128, RK45, 0.01, 4000,
+                   extra=dict(camera_distance=100.0, camera_width=60.0, camera_height=60.0, r_term_max=150.0))
+C4_CHECKPOINT_INTERVAL = 64
+C4_BACK_DISTANCE = 60.0
+
+
+def c4_target_multipliers(shape, seed=4, sigma=0.1):
+    """Seeded lognormal multiplier fields exp(N(0, sigma)) for the target image."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return np.exp(rng.normal(0.0, sigma, shape)), np.exp(rng.normal(0.0, sigma, shape))
+
+
 WORKLOADS = {"c1": C1, "c2": C2}
 BATCHES = {"c2": C2_BATCH, "c3": C3}
 

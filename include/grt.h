@@ -231,6 +231,21 @@ grt_status grt_upload_photons(grt_ctx* ctx, const grt_photon_soa* soa, size_t n)
 grt_status grt_init_image_photons(grt_ctx* ctx, uint64_t nx, uint64_t ny, uint64_t id_offset);
 
 /*
+ * Line-of-sight forward rays (no counterpart in the reference's initialisers;
+ * its functor handles them as ImageForward photons): one per pixel centre
+ * (u, v) of the camera window, starting at -back_distance * n + u th + v ph
+ * behind the scene and aimed along the camera normal n, with I = 0,
+ * frequency = custom_frequency_hz, emission_frame_energy = -p_t and
+ * dlambda = initial_step * back_distance.  They cross the fluid, accumulating
+ * emission and absorption on the way, and are binned where they cross the
+ * camera plane -- the volumetric image the adjoint differentiates (the
+ * reference's image mode emits at the first fluid contact and retraces its
+ * path outward, sampling no fluid on its forward leg).
+ */
+grt_status grt_init_image_forward_photons(grt_ctx* ctx, uint64_t nx, uint64_t ny, double back_distance,
+                                          uint64_t id_offset);
+
+/*
  * Advance the photons: equivalent to the reference's step loop for
  * step in [0, p.max_steps), stopping after the first output step
  * (step % output_interval == 0 or the last step) at which the terminated
@@ -299,6 +314,34 @@ grt_status grt_write_batch_products_npz(grt_ctx* ctx, const char* output_dir, co
  * grt_get_batch_image_products.
  */
 grt_status grt_render_graph(grt_ctx* ctx, grt_run_stats* stats);
+
+/*
+ * Differentiable radiative transfer (no counterpart in the reference).
+ * Per-cell multipliers scale the values the user extension points return:
+ * dtau = m_abs[cell] * ComputeOpticalDepthIncrement(...) and
+ * dI = m_emis[cell] * ComputeEmissivityIncrement(...)
+ * (radiative_transfer.hpp:61-96), so the gradient below is exact for any
+ * user body.  Arrays are host float64 of length nr*ntheta*nphi (C order of
+ * the grid); NULL switches that multiplier off (all ones).  Applies to every
+ * later trace (grt_run, grt_render_graph, the checkpointed forward).
+ */
+grt_status grt_set_cell_multipliers(grt_ctx* ctx, const double* m_abs, const double* m_emis);
+
+/*
+ * Trace the context's photons like grt_run (termination_percent >= 1, FP64
+ * form) and keep, per ray, its state right after the emission call and every
+ * checkpoint_interval calls after it, for grt_adjoint_image_I.
+ */
+grt_status grt_forward_checkpointed(grt_ctx* ctx, int64_t checkpoint_interval, grt_run_stats* stats);
+
+/*
+ * Adjoint of the last grt_forward_checkpointed: given dL/d(image_I) (host,
+ * [image_ny][image_nx], the binning of grt_get_image_products), write
+ * dL/dm_abs and dL/dm_emis (host, [nr*ntheta*nphi]; either may be NULL).
+ * Each ray's segments are recomputed from its checkpoints (bit-identical to
+ * the forward pass) and its radiative-transfer updates swept backwards.
+ */
+grt_status grt_adjoint_image_I(grt_ctx* ctx, const double* dL_dimage_I, double* dL_dm_abs, double* dL_dm_emis);
 
 /* Launch shape of the trace kernel. */
 grt_status grt_get_launch_config(const grt_ctx* ctx, grt_launch_config* cfg);

@@ -798,8 +798,10 @@ struct Stepper {
     }
 
     // integrate_cart_ks.hpp:230-419: one invocation on photon ph at host step `step`.
-    // trace (optional) receives the (cell, dtau_base, dI_base, I_before) of every
-    // radiative-transfer application, for the adjoint checks.
+    // trace (optional) receives (cell, dtau_base, dI_base, I_before, scale) for
+    // every radiative-transfer application -- scale = albedo when the photon
+    // scattered in that step, else 1 -- and (-1, 0, 0, 0, 0) when the Stokes
+    // vector is zeroed on arrival; the adjoint check replays it backwards.
     void call(Photon& ph, int64_t step, std::vector<real>* trace = nullptr) {
         if (ph.term) return;
         ++calls;
@@ -897,11 +899,13 @@ struct Stepper {
                 apply_rt(stokes, fluid, ph.freq, taken, abs_on, emis_on, p->absorption_coefficient,
                          p->emission_coefficient, ma, me);
             }
+            bool scattered = false;
             if (scat_on) {
                 Philox rng(p->scattering_seed + static_cast<uint64_t>(p->rank), ph.id, static_cast<uint32_t>(step));
-                maybe_scatter(s, stokes, true, p->scattering_albedo, std::fabs(ph.dl), g->length_scale,
-                              fluid, tetrad, p->spin, p->mass, rng);
+                scattered = maybe_scatter(s, stokes, true, p->scattering_albedo, std::fabs(ph.dl), g->length_scale,
+                                          fluid, tetrad, p->spin, p->mass, rng);
             }
+            if (trace && (abs_on || emis_on)) trace->push_back(scattered ? p->scattering_albedo : 1.0);
         }
         if (image && phase == GRT_PHASE_IMAGE_FORWARD) {
             real u = 0.0, v = 0.0;
@@ -913,6 +917,7 @@ struct Stepper {
                     ph.freq *= eo / ee;
                 } else {
                     stokes[0] = stokes[1] = stokes[2] = stokes[3] = 0.0;
+                    if (trace) trace->insert(trace->end(), {-1.0, 0.0, 0.0, 0.0, 0.0});
                 }
                 ph.tdisp = u;
                 ph.pdisp = v;
@@ -1184,6 +1189,59 @@ int oracle_run(const grt_params* p, size_t nr, size_t nth, size_t nph, const dou
     return 0;
 }
 
+// FP64 reference gradient of a Stokes-I image loss with respect to the
+// per-cell multipliers: every photon is stepped alone to termination (the
+// termination_percent = 1 loop), recording its radiative-transfer updates, and
+// ImageArrived photons replay them backwards from dL/dI of their pixel
+// (observation.hpp:22-29 binning over image_nx x image_ny).  photons are
+// advanced in place; g_abs/g_emis ([nr*nth*nph]) are overwritten.
+int oracle_adjoint_image_I(const grt_params* p, size_t nr, size_t nth, size_t nph, const double* r,
+                           const double* th, const double* ph, const double* rho, const double* T,
+                           const double* vel, const double* mag, const double* m_abs, const double* m_emis,
+                           grt_photon_soa* soa, size_t n, const double* dL_dI, double* g_abs, double* g_emis) {
+    Grid g = make_grid(p, nr, nth, nph, r, th, ph, rho, T, vel, mag);
+    const size_t ncell = nr * nth * nph;
+    std::vector<real> ga(ncell, 0.0), ge(ncell, 0.0);
+    Stepper st{p, &g, p->scattering_enabled && g.available, p->absorption_enabled && g.available,
+               p->emission_enabled && g.available, m_abs, m_emis};
+    st.init_camera();
+    std::vector<real> tr;
+    for (size_t i = 0; i < n; ++i) {
+        Photon pho;
+        load(soa, i, pho);
+        tr.clear();
+        for (int64_t step = 0; step < p->max_steps && !pho.term; ++step) st.call(pho, step, &tr);
+        store(pho, soa, i);
+        if (pho.phase != GRT_PHASE_IMAGE_ARRIVED) continue;
+        const auto bin = [](real v, real lo, real hi, uint64_t bins) -> uint64_t {
+            if (bins <= 1 || !(hi > lo)) return 0;
+            const real f = std::fmax(0.0, std::fmin(1.0, (v - lo) / (hi - lo)));
+            return static_cast<uint64_t>(f * static_cast<real>(bins - 1));
+        };
+        const uint64_t px = bin(pho.tdisp, -0.5 * p->camera_width, 0.5 * p->camera_width, p->image_nx);
+        const uint64_t py = bin(pho.pdisp, -0.5 * p->camera_height, 0.5 * p->camera_height, p->image_ny);
+        real lam = dL_dI[py * p->image_nx + px];
+        if (!tr.empty() && tr[tr.size() - 5] < 0.0) lam = 0.0;  // zeroed on arrival
+        for (size_t e = tr.size(); e >= 5 && lam != 0.0; e -= 5) {
+            const real* q = &tr[e - 5];
+            if (q[0] < 0.0) continue;
+            const size_t cell = static_cast<size_t>(q[0]);
+            const real tau0 = q[1], j0 = q[2], Ib = q[3], scale = q[4];
+            const real ma = m_abs ? m_abs[cell] : 1.0;
+            const real att = st.abs_on ? std::exp(-(ma * tau0)) : 1.0;
+            const real lp = lam * scale;
+            if (st.emis_on) ge[cell] += lp * j0;
+            if (st.abs_on) ga[cell] += lp * Ib * att * (-tau0);
+            lam = lp * att;
+        }
+    }
+    for (size_t c = 0; c < ncell; ++c) {
+        if (g_abs) g_abs[c] = ga[c];
+        if (g_emis) g_emis[c] = ge[c];
+    }
+    return 0;
+}
+
 // Deterministic pixel-grid variant of initialize_photons_image
 // (src/radiative_transfer/initialize_photons.hpp:82-170).
 int oracle_init_image_photons(const grt_params* p, uint64_t nx, uint64_t ny, uint64_t id_offset,
@@ -1219,6 +1277,54 @@ int oracle_init_image_photons(const grt_params* p, uint64_t nx, uint64_t ny, uin
             out->dlambda[i] = p->initial_step * D;
             out->terminate[i] = 0;
             out->phase[i] = GRT_PHASE_IMAGE_BACKWARD;
+            out->theta_disp[i] = u;
+            out->phi_disp[i] = v;
+        }
+    }
+    return 0;
+}
+
+// Line-of-sight forward rays (no counterpart in the reference initialisers;
+// the functor handles them as ImageForward photons): pixel-centre rays that
+// start on the plane -back * n behind the scene, aimed along the camera normal
+// n, with I = 0, frequency = custom_frequency_hz, emission_frame_energy = -p_t
+// and dlambda = initial_step * back.
+int oracle_init_forward_photons(const grt_params* p, uint64_t nx, uint64_t ny, double back, uint64_t id_offset,
+                                grt_photon_soa* out) {
+    const real D = p->camera_distance;
+    const real cx = D * std::sin(p->camera_theta) * std::cos(p->camera_phi);
+    const real cy = D * std::sin(p->camera_theta) * std::sin(p->camera_phi);
+    const real cz = D * std::cos(p->camera_theta);
+    const real bx = -back * std::sin(p->camera_theta) * std::cos(p->camera_phi);
+    const real by = -back * std::sin(p->camera_theta) * std::sin(p->camera_phi);
+    const real bz = -back * std::cos(p->camera_theta);
+    const real th_hat[3] = {std::cos(p->camera_theta) * std::cos(p->camera_phi),
+                            std::cos(p->camera_theta) * std::sin(p->camera_phi), -std::sin(p->camera_theta)};
+    const real ph_hat[3] = {-std::sin(p->camera_phi), std::cos(p->camera_phi), 0.0};
+    for (uint64_t iy = 0; iy < ny; ++iy) {
+        for (uint64_t ix = 0; ix < nx; ++ix) {
+            const uint64_t i = iy * nx + ix;
+            const real u = -0.5 * p->camera_width + (static_cast<real>(ix) + 0.5) * p->camera_width / static_cast<real>(nx);
+            const real v = -0.5 * p->camera_height + (static_cast<real>(iy) + 0.5) * p->camera_height / static_cast<real>(ny);
+            const real x = bx + u * th_hat[0] + v * ph_hat[0];
+            const real y = by + u * th_hat[1] + v * ph_hat[1];
+            const real z = bz + u * th_hat[2] + v * ph_hat[2];
+            real kx = cx, ky = cy, kz = cz;
+            const real kn = std::sqrt(kx * kx + ky * ky + kz * kz);
+            kx /= kn; ky /= kn; kz /= kn;
+            const real X[4] = {0.0, x, y, z};
+            const real K[3] = {kx, ky, kz};
+            real pc[4] = {0.0, 0.0, 0.0, 0.0};
+            null_covariant_momentum(X, K, p->spin, p->mass, pc);
+            out->id[i] = id_offset + i;
+            out->frequency[i] = p->custom_frequency_hz;
+            out->emission_frame_energy[i] = -pc[0];
+            out->x0[i] = 0.0; out->x1[i] = x; out->x2[i] = y; out->x3[i] = z;
+            out->k0[i] = pc[0]; out->k1[i] = pc[1]; out->k2[i] = pc[2]; out->k3[i] = pc[3];
+            out->I[i] = out->Q[i] = out->U[i] = out->V[i] = 0.0;
+            out->dlambda[i] = p->initial_step * back;
+            out->terminate[i] = 0;
+            out->phase[i] = GRT_PHASE_IMAGE_FORWARD;
             out->theta_disp[i] = u;
             out->phi_disp[i] = v;
         }

@@ -73,6 +73,10 @@ class Oracle:
         L.oracle_fourth_root_pair.restype = None
         L.oracle_observation_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint64]
         L.oracle_observation_bin.restype = C.c_uint64
+        L.oracle_init_forward_photons.argtypes = [P, C.c_uint64, C.c_uint64, C.c_double, C.c_uint64,
+                                                  C.POINTER(PhotonSoA)]
+        L.oracle_adjoint_image_I.argtypes = ([P] + [C.c_size_t] * 3 + [_DP] * 9 +
+                                             [C.POINTER(PhotonSoA), C.c_size_t, _DP, _DP, _DP])
 
     def set_pow_mode(self, mode):
         """'cr': correctly rounded controller root (kernel semantics);
@@ -84,6 +88,12 @@ class Oracle:
         ph = PhotonArrays(nx * ny)
         soa = ph.soa()
         self.lib.oracle_init_image_photons(C.byref(p), nx, ny, id_offset, C.byref(soa))
+        return ph
+
+    def init_forward_photons(self, p: Params, nx, ny, back, id_offset=0) -> PhotonArrays:
+        ph = PhotonArrays(nx * ny)
+        soa = ph.soa()
+        self.lib.oracle_init_forward_photons(C.byref(p), nx, ny, C.c_double(back), id_offset, C.byref(soa))
         return ph
 
     def run(self, p: Params, grid: dict, photons: PhotonArrays, m_abs=None, m_emis=None):
@@ -99,6 +109,25 @@ class Oracle:
         self.lib.oracle_run(C.byref(p), nr, nth, nph, *[_dp(a) for a in keep], _dp(ma), _dp(me),
                             C.byref(soa), photons.n, C.byref(st))
         return st.as_dict()
+
+    def adjoint_image_I(self, p: Params, grid: dict, photons: PhotonArrays, dL_dI, m_abs=None, m_emis=None):
+        """FP64 reference gradient of a Stokes-I image loss: traces photons in
+        place and returns (dL/dm_abs, dL/dm_emis) over the grid cells."""
+        r = grid["r.npy"]
+        nr, nth, nph = r.shape
+        keep = [np.ascontiguousarray(grid[k], dtype=np.float64) for k in
+                ("r.npy", "theta.npy", "phi.npy", "rho.npy", "Tgas.npy", "vel.npy", "mag.npy")]
+        ma = None if m_abs is None else np.ascontiguousarray(m_abs, dtype=np.float64).ravel()
+        me = None if m_emis is None else np.ascontiguousarray(m_emis, dtype=np.float64).ravel()
+        g = np.ascontiguousarray(dL_dI, dtype=np.float64)
+        if g.shape != (p.image_ny, p.image_nx):
+            raise ValueError(f"dL_dI must have shape {(p.image_ny, p.image_nx)}")
+        ga = np.zeros(nr * nth * nph)
+        ge = np.zeros(nr * nth * nph)
+        soa = photons.soa()
+        self.lib.oracle_adjoint_image_I(C.byref(p), nr, nth, nph, *[_dp(a) for a in keep], _dp(ma), _dp(me),
+                                        C.byref(soa), photons.n, _dp(g), _dp(ga), _dp(ge))
+        return ga.reshape(r.shape), ge.reshape(r.shape)
 
     def image_products(self, p: Params, photons: PhotonArrays) -> ProductArrays:
         out = ProductArrays.for_params(p)
