@@ -23,6 +23,7 @@
 #include "grt_host.h"
 #include "grt_kparams.h"
 #include "grt_launch.h"
+#include "grt_user_physics.h"
 
 namespace {
 
@@ -104,6 +105,9 @@ struct grt_ctx {
     double r_reject_lo = 0.0, r_reject_hi = 0.0;
     DevBuf<double> r_axis, th_axis, ph_axis, r_half, th_half, ph_half, r3, th3, ph3;
     DevBuf<double2> rho_t, vel, mag;
+    DevBuf<double> cell_pos;               // [ncell][3] Cartesian KS cell positions (disk emission)
+    std::vector<double> host_rho;          // code-unit density (disk packet counts)
+    DevBuf<unsigned long long> disk_offsets;
     // photons
     size_t n = 0;
     PhotonBufs ph;
@@ -348,6 +352,7 @@ void grt_destroy(grt_ctx* c) {
     c->r_half.release(); c->th_half.release(); c->ph_half.release();
     c->r3.release(); c->th3.release(); c->ph3.release();
     c->rho_t.release(); c->vel.release(); c->mag.release();
+    c->cell_pos.release(); c->disk_offsets.release();
     c->ph.release();
     c->counters.release();
     c->image.release(); c->spectrum.release(); c->arrived.release(); c->scratch_u64.release();
@@ -453,8 +458,15 @@ grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const 
         c->r_reject_hi = ra[nr - 1] * std::exp(0.6 * span_hi);
     }
     std::vector<double2> rt(ncell), uv(2 * ncell), bv(2 * ncell);
+    std::vector<double> pos(3 * ncell);
+    c->host_rho.assign(rho, rho + ncell);
     for (size_t q = 0; q < ncell; ++q) {
         rt[q] = make_double2(rho[q], T[q]);
+        // spherical_kerr_schild_to_cartesian (fluid_frame.hpp:15-26), host libm
+        const double st = std::sin(th[q]), ct = std::cos(th[q]), sp = std::sin(ph[q]), cp = std::cos(ph[q]);
+        pos[3 * q] = (r[q] * cp - c->p.spin * sp) * st;
+        pos[3 * q + 1] = (r[q] * sp + c->p.spin * cp) * st;
+        pos[3 * q + 2] = r[q] * ct;
         double u[4], b[4];
         spherical_to_cartesian_vec(r[q], th[q], ph[q], c->p.spin, vel4 + 4 * q, c->p.four_velocity_cm_s_per_code, u);
         spherical_to_cartesian_vec(r[q], th[q], ph[q], c->p.spin, mag4 + 4 * q, c->p.magnetic_gauss_per_code, b);
@@ -469,6 +481,9 @@ grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const 
     GRT_CUDA(c, c->r_axis.alloc(nr), "alloc axis");
     GRT_CUDA(c, c->th_axis.alloc(nth), "alloc axis");
     GRT_CUDA(c, c->ph_axis.alloc(nph), "alloc axis");
+    GRT_CUDA(c, c->cell_pos.alloc(3 * ncell), "alloc positions");
+    GRT_CUDA(c, cudaMemcpy(c->cell_pos.ptr, pos.data(), 3 * ncell * sizeof(double), cudaMemcpyHostToDevice),
+             "H2D positions");
     GRT_CUDA(c, cudaMemcpy(c->rho_t.ptr, rt.data(), ncell * sizeof(double2), cudaMemcpyHostToDevice), "H2D grid");
     GRT_CUDA(c, cudaMemcpy(c->vel.ptr, uv.data(), 2 * ncell * sizeof(double2), cudaMemcpyHostToDevice), "H2D grid");
     GRT_CUDA(c, cudaMemcpy(c->mag.ptr, bv.data(), 2 * ncell * sizeof(double2), cudaMemcpyHostToDevice), "H2D grid");
@@ -814,6 +829,68 @@ grt_status grt_init_image_forward_photons(grt_ctx* c, uint64_t nx, uint64_t ny, 
     if (nx * ny == 0) return fail(c, GRT_EINVAL, "nx and ny must be positive");
     const grt_image_spec sp = spec_from_params(c->p, nx, ny);
     return set_image_set(c, &sp, 1, id_offset, false, back_distance);
+}
+
+grt_status grt_init_disk_photons(grt_ctx* c, uint64_t id_offset, uint64_t* n_photons) {
+    if (!c) return GRT_EINVAL;
+    if (!c->grid_uploaded || !c->fluid_available)
+        return fail(c, GRT_ESTATE, "disk emission needs an uploaded fluid grid");
+    const grt_params& p = c->p;
+    const size_t ncell = c->host_rho.size();
+    // build_superphoton_cell_offsets (initialize_photons.hpp:32-64), on the host like the reference
+    std::vector<unsigned long long> off(ncell + 1);
+    unsigned long long total = 0;
+    for (size_t q = 0; q < ncell; ++q) {
+        off[q] = total;
+        const int count = grt::ComputeSuperphotonsPerCell(c->host_rho[q], p.superphoton_count_normalization);
+        total += static_cast<unsigned long long>(count > 0 ? count : 0);
+    }
+    off[ncell] = total;
+    if (total > (1ull << 36)) return fail(c, GRT_EINVAL, "disk packet count too large: " + std::to_string(total));
+    GRT_CUDA(c, c->ph.alloc(total), "alloc photons");
+    GRT_CUDA(c, c->disk_offsets.alloc(ncell + 1), "alloc offsets");
+    GRT_CUDA(c, cudaMemcpy(c->disk_offsets.ptr, off.data(), (ncell + 1) * sizeof(unsigned long long),
+                           cudaMemcpyHostToDevice), "H2D offsets");
+    ++c->generation;
+    c->n = total;
+    c->images.clear();
+    c->image_start.clear();
+    c->batched = false;
+    c->have_images = false;
+    c->bproducts_valid = false;
+    c->adj_ready = false;
+    grt::DiskInitArgs a{};
+    a.ph = c->ph.view();
+    a.n = total;
+    a.offsets = c->disk_offsets.ptr;
+    a.ncell = ncell;
+    a.pos = c->cell_pos.ptr;
+    a.rho_t = c->rho_t.ptr;
+    a.vel = c->vel.ptr;
+    a.mag = c->mag.ptr;
+    a.density_scale = p.density_g_cm3_per_code;
+    a.temperature_scale = p.temperature_k_per_code;
+    a.length_scale = p.length_cm_per_code;
+    a.time_scale = p.time_s_per_code;
+    a.a = p.spin;
+    a.M = p.mass;
+    a.generator = p.generator;
+    a.energy = p.energy_per_cell_erg;
+    a.pl_slope = p.power_law_slope;
+    a.nu_min = p.nu_min_hz;
+    a.nu_max = p.nu_max_hz;
+    a.nu_custom = p.custom_frequency_hz;
+    a.seed = p.scattering_seed + static_cast<uint64_t>(p.rank);
+    a.id_offset = id_offset;
+    a.dlambda0 = p.initial_step;
+    GRT_CUDA(c, grt::launch_init_disk(a, c->stream), "init_disk_photons");
+    c->initial_terminated = 0;
+    if (total > 0) {
+        grt_status st = count_initial_terminated(c);
+        if (st != GRT_OK) return st;
+    }
+    if (n_photons) *n_photons = total;
+    return GRT_OK;
 }
 
 grt_status grt_init_image_batch(grt_ctx* c, const grt_image_spec* specs, size_t nimages, uint64_t id_offset) {

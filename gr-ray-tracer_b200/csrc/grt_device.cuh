@@ -13,6 +13,7 @@
 
 #include "grt_kparams.h"
 #include "grt_metric.cuh"
+#include "grt_sincos.h"
 #include "grt_user_physics.h"
 
 namespace grt {
@@ -416,7 +417,9 @@ static __device__ __noinline__ bool maybe_scatter(ScatterState* st, double albed
     const double mu_c = 2.0 * rng.drand() - 1.0;
     const double dphi = 2.0 * kPi * rng.drand();
     const double tr = sqrt(fmax(0.0, 1.0 - mu_c * mu_c));
-    const double dx = tr * cos(dphi), dy = tr * sin(dphi), dz = mu_c;
+    double sn, cs;
+    det_sincos(dphi, &sn, &cs);  // the oracle's sin/cos bit for bit (grt_sincos.h)
+    const double dx = tr * cs, dy = tr * sn, dz = mu_c;
     double w[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) w[q] = fs.e[0][q] + dx * fs.e[1][q] + dy * fs.e[2][q] + dz * fs.e[3][q];

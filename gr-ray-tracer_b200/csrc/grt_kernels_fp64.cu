@@ -4,6 +4,7 @@
 //   trace_fp64<RK4|RK45>  -- persistent per-photon step loop (integrate_cart_ks.hpp:230-419)
 //   init_image_pixels     -- pixel-grid camera rays (initialize_photons.hpp:82-170)
 //   image_products        -- build_observation_products (observation.hpp:31-84)
+//   init_disk_photons     -- initialize_photons_disk (initialize_photons.hpp:173-327)
 //   count_terminated      -- "Count Terminated Photons" (integrate_cart_ks.hpp:496-503)
 #include "grt_launch.h"
 #include "grt_trace.cuh"
@@ -97,6 +98,93 @@ __global__ void count_terminated(const uint8_t* __restrict__ term, unsigned long
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
 
+// initialize_photons_disk (initialize_photons.hpp:173-327) for packet i: the
+// cell is the last one whose offset is <= i (locate_superphoton_cell, :66-80);
+// fluid sample, tetrad and fluid-frame magnetic field as the reference builds
+// them; frequency/energy from the configured generator; an isotropic
+// fluid-frame direction (mu, phi) lowered to p_mu.  Random draws: Philox
+// keyed by (seed, photon id, domain 0xFFFFFFFF), generator draws first, then
+// mu and phi, as in the reference.
+__global__ void init_disk_photons(const __grid_constant__ DiskInitArgs args) {
+    const unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
+    if (i >= args.n) return;
+    unsigned long long lo = 0, hi = args.ncell;
+    while (lo + 1 < hi) {
+        const unsigned long long mid = lo + (hi - lo) / 2;
+        if (args.offsets[mid] <= i) lo = mid;
+        else hi = mid;
+    }
+    const unsigned long long cell = lo;
+    const int packets = static_cast<int>(args.offsets[cell + 1] - args.offsets[cell]);
+    const double x = args.pos[3 * cell], y = args.pos[3 * cell + 1], z = args.pos[3 * cell + 2];
+    FluidCellCGS fluid;
+    fluid.position_cm[0] = x * args.length_scale;
+    fluid.position_cm[1] = y * args.length_scale;
+    fluid.position_cm[2] = z * args.length_scale;
+    fluid.coordinate_time_s = 0.0 * args.time_scale;
+    const double2 rt = args.rho_t[cell];
+    fluid.density_g_cm3 = rt.x * args.density_scale;
+    fluid.temperature_k = rt.y * args.temperature_scale;
+    const double2 u01 = args.vel[2 * cell], u23 = args.vel[2 * cell + 1];
+    fluid.coordinate_four_velocity_cm_s[0] = u01.x;
+    fluid.coordinate_four_velocity_cm_s[1] = u01.y;
+    fluid.coordinate_four_velocity_cm_s[2] = u23.x;
+    fluid.coordinate_four_velocity_cm_s[3] = u23.y;
+    const double2 b01 = args.mag[2 * cell], b23 = args.mag[2 * cell + 1];
+    const double cm[4] = {b01.x, b01.y, b23.x, b23.y};
+    dev::MetricAt m;
+    dev::ks_metric(x, y, z, args.a, args.M, m);
+    double e[4][4];
+    const bool valid = dev::build_tetrad(m.g, fluid.coordinate_four_velocity_cm_s, e);
+    fluid.magnetic_gauss[0] = fluid.magnetic_gauss[1] = fluid.magnetic_gauss[2] = fluid.magnetic_gauss[3] = 0.0;
+    if (valid) {
+        fluid.magnetic_gauss[0] = -dev::metric_dot(m.g, e[0], cm);
+        for (int axis = 1; axis < 4; ++axis) fluid.magnetic_gauss[axis] = dev::metric_dot(m.g, e[axis], cm);
+    }
+    const uint64_t id = args.id_offset + i;
+    dev::Philox rng(args.seed, id, 0xFFFFFFFFu);
+    double nu = 0.0, E = 0.0;
+    bool generated = false;
+    if (valid && args.generator == 0) {
+        generated = dev::generate_blackbody(fluid, rng, packets, args.energy, nu, E);
+    } else if (valid && args.generator == 1) {
+        generated = dev::generate_power_law(rng, packets, args.pl_slope, args.nu_min, args.nu_max, args.energy, nu, E);
+    } else if (valid) {
+        generated = GeneratePhotonsCustom(fluid, rng, packets, args.nu_custom, args.energy, nu, E);
+    }
+    const double mu = 2.0 * rng.drand() - 1.0;
+    const double dphi = 2.0 * dev::kPi * rng.drand();
+    const double tr = sqrt(fmax(0.0, 1.0 - mu * mu));
+    double sn, cs;
+    det_sincos(dphi, &sn, &cs);
+    double p[4] = {0.0, 0.0, 0.0, 0.0};
+    if (generated) {
+        double w[4];
+        for (int q = 0; q < 4; ++q) w[q] = e[0][q] + (tr * cs) * e[1][q] + (tr * sn) * e[2][q] + mu * e[3][q];
+        for (int q = 0; q < 4; ++q) {
+            double pq = 0.0;
+            for (int nn = 0; nn < 4; ++nn) pq += m.g[q][nn] * w[nn];
+            p[q] = pq;
+        }
+    }
+    double ee = 0.0;
+    if (generated)
+        for (int c = 0; c < 4; ++c) ee -= p[c] * e[0][c];
+    const KPhotons& P = args.ph;
+    P.id[i] = id;
+    P.frequency[i] = nu;
+    P.emission_frame_energy[i] = ee;
+    P.x0[i] = 0.0; P.x1[i] = x; P.x2[i] = y; P.x3[i] = z;
+    P.k0[i] = p[0]; P.k1[i] = p[1]; P.k2[i] = p[2]; P.k3[i] = p[3];
+    P.I[i] = generated ? E : 0.0;
+    P.Q[i] = 0.0; P.U[i] = 0.0; P.V[i] = 0.0;
+    P.dlambda[i] = args.dlambda0;
+    P.terminate[i] = generated ? 0 : 1;
+    P.phase[i] = generated ? 0 : 4;  // Disk / Rejected
+    P.theta_disp[i] = 0.0;
+    P.phi_disp[i] = 0.0;
+}
+
 // ---- host-side launchers ----
 template <int I, int B>
 static cudaError_t launch_trace_fp64_v(const KParams& kp, int blocks, size_t smem, cudaStream_t stream) {
@@ -132,6 +220,15 @@ cudaError_t launch_init_image(const InitImageArgs& args, cudaStream_t stream) {
     const unsigned threads = 256;
     const unsigned blocks = static_cast<unsigned>((n + threads - 1) / threads);
     init_image_pixels<<<blocks, threads, 0, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_disk(const DiskInitArgs& a, cudaStream_t stream) {
+    if (a.n == 0) return cudaSuccess;
+    const unsigned threads = 128;
+    const unsigned long long blocks = (a.n + threads - 1) / threads;
+    if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
+    init_disk_photons<<<static_cast<unsigned>(blocks), threads, 0, stream>>>(a);
     return cudaGetLastError();
 }
 

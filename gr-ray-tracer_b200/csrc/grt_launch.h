@@ -28,6 +28,27 @@ struct InitImageArgs {
     double nu0;
 };
 
+// initialize_photons_disk (initialize_photons.hpp:173-327): one photon per
+// packet; the packet's cell comes from the prefix sum of per-cell counts.
+struct DiskInitArgs {
+    KPhotons ph;
+    unsigned long long n;                // packets = offsets[ncell]
+    const unsigned long long* offsets;   // [ncell + 1]
+    unsigned long long ncell;
+    const double* pos;                   // [ncell][3] Cartesian KS cell positions (host libm)
+    const double2* rho_t;                // [ncell] (rho, T) code units
+    const double2* vel;                  // [2 * ncell] Cartesian u^mu * velocity scale
+    const double2* mag;                  // [2 * ncell] Cartesian b^mu * magnetic scale
+    double density_scale, temperature_scale, length_scale, time_scale;
+    double a, M;
+    int generator;
+    int pad;
+    double energy, pl_slope, nu_min, nu_max, nu_custom;
+    uint64_t seed;                       // scattering seed + rank (Philox key)
+    unsigned long long id_offset;
+    double dlambda0;                     // initial_step (disk mode: unscaled)
+};
+
 struct ProductsArgs {
     KPhotons ph;
     unsigned long long offset, n;  // photon slots [offset, offset + n)
@@ -99,6 +120,7 @@ cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int sm_count, i
 cudaError_t launch_trace_mixed(const KParams& kp, int integrator, int sm_count, int blocks_per_sm, size_t smem,
                                cudaStream_t stream);
 cudaError_t launch_init_image(const InitImageArgs& args, cudaStream_t stream);
+cudaError_t launch_init_disk(const DiskInitArgs& a, cudaStream_t stream);
 cudaError_t launch_image_products(const ProductsArgs& args, cudaStream_t stream);
 cudaError_t launch_count_terminated(const uint8_t* term, unsigned long long n, unsigned long long* out,
                                     int sm_count, cudaStream_t stream);

@@ -22,7 +22,7 @@ from __future__ import annotations
 import math
 from dataclasses import dataclass, field
 
-from .abi import GEN_CUSTOM, MODE_IMAGE, PREC_FP64, RK4, RK45, ImageSpec, Params
+from .abi import GEN_BLACKBODY, GEN_CUSTOM, MODE_DISK, MODE_IMAGE, PREC_FP64, RK4, RK45, ImageSpec, Params
 from .config import reference_defaults
 
 
@@ -139,6 +139,50 @@ def c4_target_multipliers(shape, seed=4, sigma=0.1):
     import numpy as np
     rng = np.random.default_rng(seed)
     return np.exp(rng.normal(0.0, sigma, shape)), np.exp(rng.normal(0.0, sigma, shape))
+
+
+@dataclass
+class DiskWorkload:
+    """Disk-mode scattering Monte Carlo (grt_init_disk_photons): packets from
+    every torus cell, RK45, elastic (albedo 1) isotropic scattering in the
+    fluid frame, absorption and emission on.  The Thomson optical depth across
+    the torus is ~1 through the unit scales (scattering.optical_depth is not
+    read by the reference): tau = sigma_T / m_p * rho_code * density_scale *
+    path_code * length_scale ~ 0.4 * 0.5 * 0.5 * 10 = 1 for a 10 M chord at
+    rho_code ~ 0.5.  Escape is termination beyond r_term_max."""
+    name: str
+    grid: tuple
+    spin: float
+    normalization: float
+    r_escape: float = 100.0
+    rtol: float = 1e-8
+    initial_step: float = 0.01
+    max_steps: int = 20000
+    kappa: float = 0.1
+    jcoef: float = 1e-10
+
+    def params(self) -> Params:
+        p = reference_defaults()
+        horizon = 1.0 + math.sqrt(max(0.0, 1.0 - self.spin * self.spin))
+        p.update(mode=MODE_DISK, integrator=RK45, precision=PREC_FP64, generator=GEN_BLACKBODY,
+                 mass=1.0, spin=self.spin, r_term_min=horizon, r_term_max=self.r_escape,
+                 atol=self.rtol, rtol=self.rtol, max_steps=self.max_steps, termination_percent=1.0,
+                 output_interval=10**9, initial_step=self.initial_step,
+                 absorption_enabled=1, emission_enabled=1, absorption_coefficient=self.kappa,
+                 emission_coefficient=self.jcoef, scattering_enabled=1, scattering_albedo=1.0,
+                 scattering_seed=2024, superphoton_count_normalization=self.normalization,
+                 energy_per_cell_erg=1.0, density_g_cm3_per_code=0.5, length_cm_per_code=1.0,
+                 temperature_k_per_code=1e11, camera_distance=self.r_escape)
+        return p
+
+    def torus(self):
+        from .torus import benchmark_torus
+        return benchmark_torus(*self.grid, spin=self.spin)
+
+
+# 1e7 packets (normalisation 210 on the 128x64x64 torus: sum of int(rho * 210)
+# over the cells), a = 0.9.
+C5 = DiskWorkload("c5_disk_1e7", (128, 64, 64), 0.9, 210.0)
 
 
 WORKLOADS = {"c1": C1, "c2": C2}

@@ -268,6 +268,18 @@ grt_status grt_get_image_products(grt_ctx* ctx, grt_image_products* out);
 grt_status grt_write_image_products_npz(grt_ctx* ctx, const char* output_dir, const char* name);
 
 /*
+ * Disk-mode emission, as initialize_photons_disk (initialize_photons.hpp:
+ * 173-327) after build_superphoton_cell_offsets (:32-64): every grid cell
+ * emits ComputeSuperphotonsPerCell(rho, superphoton_count_normalization)
+ * packets from its centre, with the generator's frequency and energy and an
+ * isotropic fluid-frame direction; packets whose cell has no valid fluid tetrad
+ * or whose generator fails start Rejected.  Random draws use Philox keyed by
+ * (scattering_seed + rank, photon id).  Replaces the context's photons;
+ * *n_photons (may be NULL) receives the packet count.
+ */
+grt_status grt_init_disk_photons(grt_ctx* ctx, uint64_t id_offset, uint64_t* n_photons);
+
+/*
  * Batched image mode (no counterpart in the reference, which renders one
  * camera per run): several images, each with its own camera and radiative
  * coefficients (inclinations, resolutions, frequency channels), traced by ONE

@@ -23,6 +23,7 @@
 
 #include "grt.h"
 #include "grt_fourth_root.cuh"  // the product's controller root, checked below against cr::fourth_root
+#include "grt_sincos.h"        // deterministic sin/cos shared with the kernels (scattering directions)
 #include "grt_user_physics.h"
 
 namespace oracle {
@@ -626,7 +627,9 @@ bool maybe_scatter(real state[8], real stokes[4], bool enabled, real albedo, rea
     const real tr = std::sqrt(std::fmax(real(0.0), 1.0 - mu_c * mu_c));
     const real pos[4] = {state[IT], state[IX], state[IY], state[IZ]};
     real pm[4];
-    fluid_direction_to_momentum(pos, e, tr * std::cos(dphi), tr * std::sin(dphi), mu_c, spin, mass, pm);
+    real sn, cs;
+    grt::det_sincos(dphi, &sn, &cs);  // the kernels' sin/cos (grt_sincos.h), libm within 1 ulp
+    fluid_direction_to_momentum(pos, e, tr * cs, tr * sn, mu_c, spin, mass, pm);
     for (int q = 0; q < 4; ++q) state[IKT + q] = E * pm[q];
     stokes[0] *= albedo;
     stokes[1] *= 0.5 * albedo;
@@ -1242,6 +1245,102 @@ int oracle_adjoint_image_I(const grt_params* p, size_t nr, size_t nth, size_t np
     return 0;
 }
 
+// initialize_photons_disk (src/radiative_transfer/initialize_photons.hpp:
+// 173-327) after build_superphoton_cell_offsets (:32-64), with the kernels'
+// random streams (Philox keyed by seed + rank, photon id, domain 0xFFFFFFFF;
+// generator draws, then mu, phi) and the shared deterministic sin/cos for the
+// direction.  out == NULL only counts the packets (*n_out).
+int oracle_init_disk_photons(const grt_params* p, size_t nr, size_t nth, size_t nph, const double* r,
+                             const double* th, const double* ph, const double* rho, const double* T,
+                             const double* vel, const double* mag, uint64_t id_offset, grt_photon_soa* out,
+                             uint64_t* n_out) {
+    Grid g = make_grid(p, nr, nth, nph, r, th, ph, rho, T, vel, mag);
+    const size_t ncell = nr * nth * nph;
+    std::vector<uint64_t> off(ncell + 1);
+    uint64_t total = 0;
+    for (size_t c = 0; c < ncell; ++c) {
+        off[c] = total;
+        const int count = grt::ComputeSuperphotonsPerCell(rho[c], p->superphoton_count_normalization);
+        total += static_cast<uint64_t>(count > 0 ? count : 0);
+    }
+    off[ncell] = total;
+    if (n_out) *n_out = total;
+    if (!out) return 0;
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < static_cast<int64_t>(total); ++ii) {
+        const uint64_t i = static_cast<uint64_t>(ii);
+        size_t lo = 0, hi = ncell;  // locate_superphoton_cell (:66-80)
+        while (lo + 1 < hi) {
+            const size_t mid = lo + (hi - lo) / 2;
+            if (off[mid] <= i) lo = mid;
+            else hi = mid;
+        }
+        const size_t c = lo;
+        const int packets = static_cast<int>(off[c + 1] - off[c]);
+        real pos[4];
+        spherical_to_cartesian(r[c], th[c], ph[c], p->spin, pos);
+        FluidCellCGS fluid;
+        for (int q = 0; q < 3; ++q) fluid.position_cm[q] = pos[q + 1] * g.length_scale;
+        fluid.coordinate_time_s = pos[0] * g.time_scale;
+        fluid.density_g_cm3 = rho[c] * g.density_scale;
+        fluid.temperature_k = T[c] * g.temperature_scale;
+        real sv[4], sm[4], cm[4];
+        for (int q = 0; q < 4; ++q) {
+            sv[q] = vel[4 * c + q];
+            sm[q] = mag[4 * c + q];
+        }
+        spherical_vector_to_cartesian(r[c], th[c], ph[c], p->spin, sv, fluid.coordinate_four_velocity_cm_s);
+        for (int q = 0; q < 4; ++q) fluid.coordinate_four_velocity_cm_s[q] *= g.velocity_scale;
+        spherical_vector_to_cartesian(r[c], th[c], ph[c], p->spin, sm, cm);
+        for (int q = 0; q < 4; ++q) cm[q] *= g.magnetic_scale;
+        real e[4][4];
+        const bool valid = build_fluid_tetrad(pos, fluid.coordinate_four_velocity_cm_s, p->spin, p->mass, e);
+        for (int q = 0; q < 4; ++q) fluid.magnetic_gauss[q] = 0.0;
+        if (valid) {
+            real metric[4][4];
+            compute_metric(pos, p->spin, p->mass, metric);
+            fluid.magnetic_gauss[0] = -metric_inner_product(metric, e[0], cm);
+            for (int axis = 1; axis < 4; ++axis) fluid.magnetic_gauss[axis] = metric_inner_product(metric, e[axis], cm);
+        }
+        const uint64_t id = id_offset + i;
+        Philox rng(p->scattering_seed + static_cast<uint64_t>(p->rank), id, 0xFFFFFFFFu);
+        real nu = 0.0, E = 0.0;
+        bool generated = false;
+        if (valid && p->generator == GRT_GEN_BLACKBODY) {
+            generated = generate_blackbody(fluid, rng, packets, p->energy_per_cell_erg, nu, E);
+        } else if (valid && p->generator == GRT_GEN_POWER_LAW) {
+            generated = generate_power_law(rng, packets, p->power_law_slope, p->nu_min_hz, p->nu_max_hz,
+                                           p->energy_per_cell_erg, nu, E);
+        } else if (valid) {
+            generated = grt::GeneratePhotonsCustom(fluid, rng, packets, p->custom_frequency_hz, p->energy_per_cell_erg,
+                                                   nu, E);
+        }
+        const real mu = 2.0 * rng.drand() - 1.0;
+        const real dphi = 2.0 * PI * rng.drand();
+        const real tr = std::sqrt(std::fmax(real(0.0), 1.0 - mu * mu));
+        real sn, cs;
+        grt::det_sincos(dphi, &sn, &cs);
+        real pc[4] = {0.0, 0.0, 0.0, 0.0};
+        if (generated) fluid_direction_to_momentum(pos, e, tr * cs, tr * sn, mu, p->spin, p->mass, pc);
+        real ee = 0.0;
+        if (generated)
+            for (int q = 0; q < 4; ++q) ee -= pc[q] * e[0][q];
+        out->id[i] = id;
+        out->frequency[i] = nu;
+        out->emission_frame_energy[i] = ee;
+        out->x0[i] = pos[0]; out->x1[i] = pos[1]; out->x2[i] = pos[2]; out->x3[i] = pos[3];
+        out->k0[i] = pc[0]; out->k1[i] = pc[1]; out->k2[i] = pc[2]; out->k3[i] = pc[3];
+        out->I[i] = generated ? E : 0.0;
+        out->Q[i] = out->U[i] = out->V[i] = 0.0;
+        out->dlambda[i] = p->initial_step;
+        out->terminate[i] = generated ? 0 : 1;
+        out->phase[i] = generated ? GRT_PHASE_DISK : GRT_PHASE_REJECTED;
+        out->theta_disp[i] = 0.0;
+        out->phi_disp[i] = 0.0;
+    }
+    return 0;
+}
+
 // Deterministic pixel-grid variant of initialize_photons_image
 // (src/radiative_transfer/initialize_photons.hpp:82-170).
 int oracle_init_image_photons(const grt_params* p, uint64_t nx, uint64_t ny, uint64_t id_offset,
@@ -1442,6 +1541,9 @@ double oracle_philox_drand(uint64_t seed, uint64_t id, uint32_t domain, int inde
     return d;
 }
 void oracle_set_pow_mode(int mode) { g_pow_mode = mode; }
+void oracle_det_sincos(const double* x, uint64_t n, double* s, double* c) {
+    for (uint64_t i = 0; i < n; ++i) grt::det_sincos(x[i], s + i, c + i);
+}
 double oracle_fourth_root(double x) { return cr::fourth_root(x); }
 // Element-wise: out_oracle[i] = the oracle's arbitrary-precision root,
 // out_product[i] = the product's fourth_root_cr (rounding test + 256-bit

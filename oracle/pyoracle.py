@@ -73,6 +73,10 @@ class Oracle:
         L.oracle_fourth_root_pair.restype = None
         L.oracle_observation_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint64]
         L.oracle_observation_bin.restype = C.c_uint64
+        L.oracle_init_disk_photons.argtypes = ([P] + [C.c_size_t] * 3 + [_DP] * 7 +
+                                               [C.c_uint64, C.POINTER(PhotonSoA), C.POINTER(C.c_uint64)])
+        L.oracle_det_sincos.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.oracle_det_sincos.restype = None
         L.oracle_init_forward_photons.argtypes = [P, C.c_uint64, C.c_uint64, C.c_double, C.c_uint64,
                                                   C.POINTER(PhotonSoA)]
         L.oracle_adjoint_image_I.argtypes = ([P] + [C.c_size_t] * 3 + [_DP] * 9 +
@@ -88,6 +92,20 @@ class Oracle:
         ph = PhotonArrays(nx * ny)
         soa = ph.soa()
         self.lib.oracle_init_image_photons(C.byref(p), nx, ny, id_offset, C.byref(soa))
+        return ph
+
+    def init_disk_photons(self, p: Params, grid: dict, id_offset=0) -> PhotonArrays:
+        r = grid["r.npy"]
+        nr, nth, nph = r.shape
+        keep = [np.ascontiguousarray(grid[k], dtype=np.float64) for k in
+                ("r.npy", "theta.npy", "phi.npy", "rho.npy", "Tgas.npy", "vel.npy", "mag.npy")]
+        n = C.c_uint64(0)
+        self.lib.oracle_init_disk_photons(C.byref(p), nr, nth, nph, *[_dp(a) for a in keep], id_offset, None,
+                                          C.byref(n))
+        ph = PhotonArrays(n.value)
+        soa = ph.soa()
+        self.lib.oracle_init_disk_photons(C.byref(p), nr, nth, nph, *[_dp(a) for a in keep], id_offset,
+                                          C.byref(soa), C.byref(n))
         return ph
 
     def init_forward_photons(self, p: Params, nx, ny, back, id_offset=0) -> PhotonArrays:
@@ -167,6 +185,8 @@ class Reference:
         L.ref_init_image_photons.argtypes = [C.c_char_p, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(PhotonSoA)]
         L.ref_run_photons.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(PhotonSoA), C.c_uint64,
                                       C.POINTER(ImageProducts), _DP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.ref_init_disk_photons.argtypes = [C.c_char_p, C.c_char_p, C.c_uint64, C.POINTER(PhotonSoA),
+                                            C.POINTER(C.c_uint64)]
         L.ref_hamiltonian_rhs.argtypes = [_DP, _DP, C.c_double, C.c_double, _DP]
         L.ref_null_momentum.argtypes = [_DP, _DP, C.c_double, C.c_double, _DP]
         L.ref_inverse_metric_deriv.argtypes = [_DP, C.c_double, C.c_double, _DP]
@@ -190,6 +210,18 @@ class Reference:
         ph = PhotonArrays(nx * ny)
         soa = ph.soa()
         if self.lib.ref_init_image_photons(str(toml).encode(), nx, ny, id_offset, C.byref(soa)) != 0:
+            raise ValueError(self.error())
+        return ph
+
+    def init_disk_photons(self, toml, numpy_dir=None, id_offset=0) -> PhotonArrays:
+        """The reference's own disk-mode emission (its cell offsets and initialiser)."""
+        nd = str(numpy_dir).encode() if numpy_dir else None
+        n = C.c_uint64(0)
+        if self.lib.ref_init_disk_photons(str(toml).encode(), nd, id_offset, None, C.byref(n)) != 0:
+            raise ValueError(self.error())
+        ph = PhotonArrays(n.value)
+        soa = ph.soa()
+        if self.lib.ref_init_disk_photons(str(toml).encode(), nd, id_offset, C.byref(soa), C.byref(n)) != 0:
             raise ValueError(self.error())
         return ph
 

@@ -289,6 +289,34 @@ int ref_run_photons(const char* toml_path, const char* numpy_dir_override, const
     }
 }
 
+// The reference's own disk-mode emission: build_superphoton_cell_offsets +
+// initialize_photons_disk (src/radiative_transfer/initialize_photons.hpp:
+// 32-64,173-327) on the config's grid, with the shim's random pool (its own
+// XorShift streams, not Kokkos's).  out == NULL only counts the packets.
+int ref_init_disk_photons(const char* toml_path, const char* numpy_dir_override, std::uint64_t id_offset,
+                          grt_photon_soa* out, std::uint64_t* n_out) {
+    Loaded cfg;
+    if (!load_config(toml_path, cfg)) return 1;
+    try {
+        if (numpy_dir_override) cfg.options.numpy_dir = numpy_dir_override;
+        const NumpyFieldPaths paths = discover_numpy_field_paths(cfg.options.numpy_dir);
+        NumpyFieldViews fields = load_numpy_field_bundle(paths, cfg.decomposition, 0, 1);
+        const SuperphotonCellOffsets offsets =
+            build_superphoton_cell_offsets(fields.density, cfg.generation.superphoton_count_normalization);
+        if (n_out) *n_out = offsets.total_photons;
+        if (!out) return 0;
+        Photons photons(static_cast<int>(offsets.total_photons), "photons_");
+        initialize_photons_disk(static_cast<int>(offsets.total_photons), 0, id_offset, fields.r, fields.theta,
+                                fields.phi, fields.density, fields.temperature, fields.velocity, fields.magnetic,
+                                cfg.generation, cfg.units, offsets.offsets, photons);
+        to_soa(photons, out);
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 2;
+    }
+}
+
 // ---- reference functions exposed for known-answer checks ----
 void ref_hamiltonian_rhs(const double X[4], const double p[4], double a, double M, double rhs[8]) {
     kerr_schild::compute_hamiltonian_rhs(X, p, a, M, rhs);

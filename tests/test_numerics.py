@@ -68,3 +68,22 @@ def test_product_fourth_root_matches_oracle(oracle):
     oracle.lib.oracle_fourth_root_pair(x.ctypes.data, C.c_uint64(x.size), a.ctypes.data, b.ctypes.data)
     bad = np.flatnonzero(a.view(np.uint64) != b.view(np.uint64))
     assert bad.size == 0, x[bad[:5]]
+
+
+def test_deterministic_sincos_accuracy(oracle):
+    """grt_sincos.h (scattering and emission directions, shared by the kernels
+    and the oracle): within 1.2e-16 absolute of sin/cos on [0, 2 pi], and at
+    most 1 ulp where |value| > 1e-3 (mpmath at 120 bits on a sample)."""
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.prec = 120
+    rng = np.random.default_rng(5)
+    x = np.concatenate([rng.uniform(0.0, 2.0 * np.pi, 4000),
+                        np.array([0.0, np.pi / 4, np.pi / 2, np.pi, 1.5 * np.pi, 2.0 * np.pi - 1e-12])])
+    s = np.empty_like(x)
+    c = np.empty_like(x)
+    oracle.lib.oracle_det_sincos(x.ctypes.data, C.c_uint64(x.size), s.ctypes.data, c.ctypes.data)
+    for xi, si, ci in zip(x, s, c):
+        for got, want in ((si, float(mpmath.sin(xi))), (ci, float(mpmath.cos(xi)))):
+            assert abs(got - want) <= 1.2e-16, (xi, got, want)
+            if abs(want) > 1e-3:
+                assert abs(got - want) <= np.spacing(abs(want)), (xi, got, want)
