@@ -128,6 +128,7 @@ struct grt_ctx {
     std::vector<unsigned long long> image_start;
     uint64_t image_id_offset = 0;
     double forward_back = 0.0;  // > 0: line-of-sight forward rays from -forward_back * n
+    uint64_t row0 = 0, nrows = 0;  // single image: pixel rows [row0, row0 + nrows) only (nrows 0 = all)
     bool batched = false;      // trace kernels read the per-image table
     bool have_images = false;  // photons came from an image init (a render can re-initialise them)
     DevBuf<grt::KImage> images_dev;
@@ -633,6 +634,9 @@ grt_status launch_image_inits(grt_ctx* c) {
         a.offset = c->image_start[k];
         a.nx = sp.nx;
         a.ny = sp.ny;
+        a.row0 = c->nrows ? c->row0 : 0;
+        a.nrows = c->nrows ? c->nrows : sp.ny;
+        // ids: image k's pixel (ix, iy) is id_offset + start_k + iy * nx + ix
         a.id_offset = c->image_id_offset + c->image_start[k];
         a.W = sp.camera_width;
         a.H = sp.camera_height;
@@ -664,7 +668,7 @@ grt_status launch_image_inits(grt_ctx* c) {
 }
 
 grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages, uint64_t id_offset, bool batched,
-                         double forward_back = 0.0) {
+                         double forward_back = 0.0, uint64_t row0 = 0, uint64_t nrows = 0) {
     unsigned long long total = 0;
     std::vector<unsigned long long> start(nimages + 1, 0);
     for (size_t k = 0; k < nimages; ++k) {
@@ -676,7 +680,7 @@ grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages
             return fail(c, GRT_EINVAL, "image " + std::to_string(k) +
                                            ": camera distance, width and height must be positive and angles finite");
         start[k] = total;
-        total += sp.nx * sp.ny;
+        total += sp.nx * (nrows ? nrows : sp.ny);
         if (total > (1ull << 40)) return fail(c, GRT_EINVAL, "photon count too large");
     }
     start[nimages] = total;
@@ -688,6 +692,8 @@ grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages
     c->image_start = start;
     c->image_id_offset = id_offset;
     c->forward_back = forward_back;
+    c->row0 = row0;
+    c->nrows = nrows;
     c->batched = batched;
     c->have_images = true;
     c->bproducts_valid = false;
@@ -819,6 +825,15 @@ grt_status grt_init_image_photons(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t
         return GRT_OK;
     }
     return set_image_set(c, &sp, 1, id_offset, false);
+}
+
+grt_status grt_init_image_rows(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t row0, uint64_t nrows,
+                               uint64_t id_offset) {
+    if (!c) return GRT_EINVAL;
+    if (nx == 0 || ny == 0 || nrows == 0 || row0 >= ny || nrows > ny - row0)
+        return fail(c, GRT_EINVAL, "rows [row0, row0 + nrows) must lie inside the ny-row screen");
+    const grt_image_spec sp = spec_from_params(c->p, nx, ny);
+    return set_image_set(c, &sp, 1, id_offset, false, 0.0, row0, nrows);
 }
 
 grt_status grt_init_image_forward_photons(grt_ctx* c, uint64_t nx, uint64_t ny, double back_distance,

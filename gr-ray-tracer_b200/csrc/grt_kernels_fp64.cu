@@ -27,8 +27,8 @@ __global__ void __launch_bounds__(128, MINB) trace_fp64(const __grid_constant__ 
 // With args.forward, line-of-sight forward rays instead (see InitImageArgs).
 __global__ void init_image_pixels(const __grid_constant__ InitImageArgs args) {
     const unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
-    if (i >= args.nx * args.ny) return;
-    const unsigned long long iy = i / args.nx, ix = i % args.nx;
+    if (i >= args.nx * args.nrows) return;
+    const unsigned long long iy = args.row0 + i / args.nx, ix = i % args.nx;
     const double u = -0.5 * args.W + (static_cast<double>(ix) + 0.5) * args.W / static_cast<double>(args.nx);
     const double v = -0.5 * args.H + (static_cast<double>(iy) + 0.5) * args.H / static_cast<double>(args.ny);
     const bool fwd = args.forward != 0;
@@ -46,7 +46,7 @@ __global__ void init_image_pixels(const __grid_constant__ InitImageArgs args) {
     dev::ks_null_momentum(X, K, args.a, args.M, p);
     const KPhotons& P = args.ph;
     const unsigned long long o = args.offset + i;
-    P.id[o] = args.id_offset + i;
+    P.id[o] = args.id_offset + args.row0 * args.nx + i;
     P.frequency[o] = fwd ? args.nu0 : 0.0;
     P.emission_frame_energy[o] = fwd ? -p[0] : 1.0;
     P.x0[o] = 0.0; P.x1[o] = x; P.x2[o] = y; P.x3[o] = z;
@@ -215,7 +215,7 @@ cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int sm_count, i
 }
 
 cudaError_t launch_init_image(const InitImageArgs& args, cudaStream_t stream) {
-    const unsigned long long n = args.nx * args.ny;
+    const unsigned long long n = args.nx * args.nrows;
     if (n == 0) return cudaSuccess;
     const unsigned threads = 256;
     const unsigned blocks = static_cast<unsigned>((n + threads - 1) / threads);

@@ -15,6 +15,7 @@ struct InitImageArgs {
     KPhotons ph;
     unsigned long long offset;     // first photon slot written
     unsigned long long nx, ny;
+    unsigned long long row0, nrows;  // pixel rows [row0, row0 + nrows) of the ny-row screen
     unsigned long long id_offset;
     double W, H;
     double cx, cy, cz;

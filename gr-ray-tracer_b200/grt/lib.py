@@ -83,6 +83,8 @@ def load(path: Path | None = None):
     L.grt_get_batch_image_products.argtypes = [vp, C.c_size_t, P(ImageProducts)]
     L.grt_write_batch_products_npz.argtypes = [vp, C.c_char_p, C.c_char_p]
     L.grt_render_graph.argtypes = [vp, P(RunStats)]
+    L.grt_init_image_rows.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]
+    L.grt_init_image_rows.restype = C.c_int
     L.grt_init_disk_photons.argtypes = [vp, C.c_uint64, P(C.c_uint64)]
     L.grt_init_disk_photons.restype = C.c_int
     L.grt_init_image_forward_photons.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_double, C.c_uint64]
@@ -219,6 +221,10 @@ class Context:
 
     def init_image_photons(self, nx, ny, id_offset=0):
         self._check(self.lib.grt_init_image_photons(self._h, nx, ny, id_offset))
+
+    def init_image_rows(self, nx, ny, row0, nrows, id_offset=0):
+        """Pixel rows [row0, row0 + nrows) of the nx x ny screen (one image split across ranks)."""
+        self._check(self.lib.grt_init_image_rows(self._h, nx, ny, row0, nrows, id_offset))
 
     def init_disk_photons(self, id_offset=0) -> int:
         """Disk-mode packets from every grid cell (initialize_photons_disk); returns their count."""

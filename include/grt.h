@@ -231,6 +231,16 @@ grt_status grt_upload_photons(grt_ctx* ctx, const grt_photon_soa* soa, size_t n)
 grt_status grt_init_image_photons(grt_ctx* ctx, uint64_t nx, uint64_t ny, uint64_t id_offset);
 
 /*
+ * The pixel rows [row0, row0 + nrows) of the nx*ny screen of
+ * grt_init_image_photons (same rays, same ids id_offset + iy*nx + ix): one
+ * image split across GPUs, each rank tracing its rows; every rank's
+ * grt_get_image_products covers the full image, so summing them over the
+ * ranks gives the single-GPU products.
+ */
+grt_status grt_init_image_rows(grt_ctx* ctx, uint64_t nx, uint64_t ny, uint64_t row0, uint64_t nrows,
+                               uint64_t id_offset);
+
+/*
  * Line-of-sight forward rays (no counterpart in the reference's initialisers;
  * its functor handles them as ImageForward photons): one per pixel centre
  * (u, v) of the camera window, starting at -back_distance * n + u th + v ph
