@@ -133,6 +133,14 @@ struct grt_ctx {
     bool have_images = false;  // photons came from an image init (a render can re-initialise them)
     DevBuf<grt::KImage> images_dev;
     DevBuf<unsigned long long> image_start_dev;
+    // channel groups of the batch: images with the same camera and screen
+    // share one geodesic per pixel (when scattering is off)
+    bool share_channels = true;
+    int ngroups = 0;
+    bool groups_share = false;            // some group has two or more channels
+    unsigned long long geodesics = 0;     // queue length with sharing
+    DevBuf<unsigned long long> group_qstart_dev;
+    DevBuf<int> group_chan_dev, chan_img_dev;
     // per-image products of a batch: image k's I,Q,U,V at bimage + bimage_off[k]
     DevBuf<double> bimage, bspectrum;
     DevBuf<unsigned long long> barrived;
@@ -295,6 +303,15 @@ grt::KParams make_kparams(const grt_ctx* c) {
     }
     k.ph = c->ph.view();
     k.n = c->n;
+    // Frequency channels share their geodesic when nothing channel-specific
+    // can change it: no scattering (its draws are keyed by each photon's id).
+    if (c->batched && c->share_channels && c->groups_share && !k.scat_on) {
+        k.ngroups = c->ngroups;
+        k.group_qstart = c->group_qstart_dev.ptr;
+        k.group_chan = c->group_chan_dev.ptr;
+        k.chan_img = c->chan_img_dev.ptr;
+        k.n = c->geodesics;
+    }
     k.counters = c->counters.ptr;
     k.refill_threshold = c->lc.refill_threshold;
     k.grab = c->lc.photons_per_grab;
@@ -358,6 +375,7 @@ void grt_destroy(grt_ctx* c) {
     c->counters.release();
     c->image.release(); c->spectrum.release(); c->arrived.release(); c->scratch_u64.release();
     c->images_dev.release(); c->image_start_dev.release();
+    c->group_qstart_dev.release(); c->group_chan_dev.release(); c->chan_img_dev.release();
     c->m_abs.release(); c->m_emis.release();
     c->ckpt.release(); c->tape.release(); c->dLdI.release(); c->g_abs.release(); c->g_emis.release();
     c->nckpt.release(); c->adj_overflow.release(); c->call0.release();
@@ -714,6 +732,46 @@ grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages
                  "H2D image table");
         GRT_CUDA(c, cudaMemcpy(c->image_start_dev.ptr, start.data(), (nimages + 1) * sizeof(unsigned long long),
                                cudaMemcpyHostToDevice), "H2D image table");
+        // channel groups: same camera plane and screen (exact parameter equality)
+        std::vector<std::vector<int>> groups;
+        for (size_t k = 0; k < nimages; ++k) {
+            const grt_image_spec& a = specs[k];
+            bool placed = false;
+            for (auto& g : groups) {
+                const grt_image_spec& b = specs[g[0]];
+                if (a.camera_theta == b.camera_theta && a.camera_phi == b.camera_phi &&
+                    a.camera_distance == b.camera_distance && a.camera_width == b.camera_width &&
+                    a.camera_height == b.camera_height && a.nx == b.nx && a.ny == b.ny && g.size() < 32) {
+                    g.push_back(static_cast<int>(k));
+                    placed = true;
+                    break;
+                }
+            }
+            if (!placed) groups.push_back({static_cast<int>(k)});
+        }
+        std::vector<unsigned long long> qstart(groups.size() + 1, 0);
+        std::vector<int> gchan(groups.size() + 1, 0), chan;
+        c->groups_share = false;
+        for (size_t g = 0; g < groups.size(); ++g) {
+            qstart[g + 1] = qstart[g] + specs[groups[g][0]].nx * specs[groups[g][0]].ny;
+            gchan[g + 1] = gchan[g] + static_cast<int>(groups[g].size());
+            chan.insert(chan.end(), groups[g].begin(), groups[g].end());
+            if (groups[g].size() > 1) c->groups_share = true;
+        }
+        c->ngroups = static_cast<int>(groups.size());
+        c->geodesics = qstart.back();
+        GRT_CUDA(c, c->group_qstart_dev.alloc(qstart.size()), "alloc groups");
+        GRT_CUDA(c, c->group_chan_dev.alloc(gchan.size()), "alloc groups");
+        GRT_CUDA(c, c->chan_img_dev.alloc(chan.size()), "alloc groups");
+        GRT_CUDA(c, cudaMemcpy(c->group_qstart_dev.ptr, qstart.data(), qstart.size() * sizeof(unsigned long long),
+                               cudaMemcpyHostToDevice), "H2D groups");
+        GRT_CUDA(c, cudaMemcpy(c->group_chan_dev.ptr, gchan.data(), gchan.size() * sizeof(int), cudaMemcpyHostToDevice),
+                 "H2D groups");
+        GRT_CUDA(c, cudaMemcpy(c->chan_img_dev.ptr, chan.data(), chan.size() * sizeof(int), cudaMemcpyHostToDevice),
+                 "H2D groups");
+    } else {
+        c->ngroups = 0;
+        c->groups_share = false;
     }
     return launch_image_inits(c);
 }
@@ -916,6 +974,13 @@ grt_status grt_init_image_batch(grt_ctx* c, const grt_image_spec* specs, size_t 
 }
 
 size_t grt_batch_image_count(const grt_ctx* c) { return c && c->batched ? c->images.size() : 0; }
+
+grt_status grt_set_channel_sharing(grt_ctx* c, int enable) {
+    if (!c) return GRT_EINVAL;
+    c->share_channels = enable != 0;
+    ++c->generation;
+    return GRT_OK;
+}
 
 grt_status grt_get_batch_image_products(grt_ctx* c, size_t image, grt_image_products* out) {
     if (!c || !out) return GRT_EINVAL;

@@ -13,13 +13,13 @@ namespace grt {
 
 // 128-thread blocks; MINB resident blocks per SM caps the registers per
 // thread at 65536 / (128 * MINB): 255, 170 and 128 for MINB = 2, 3, 4.
-template <int INTEGRATOR, int MINB>
+template <int INTEGRATOR, int MINB, bool SHARE>
 __global__ void __launch_bounds__(128, MINB) trace_fp64(const __grid_constant__ KParams kp) {
     extern __shared__ double smem[];
     dev::Axes ax;
     dev::KStore kk;
     dev::stage_grid(kp, smem, INTEGRATOR, ax, kk);
-    dev::trace_body<INTEGRATOR, dev::Fp64Rhs>(kp, ax, kk);
+    dev::trace_body<INTEGRATOR, dev::Fp64Rhs, false, SHARE>(kp, ax, kk);
 }
 
 // initialize_photons.hpp:116-169 with screen (u, v) at pixel centres; the
@@ -188,8 +188,13 @@ __global__ void init_disk_photons(const __grid_constant__ DiskInitArgs args) {
 // ---- host-side launchers ----
 template <int I, int B>
 static cudaError_t launch_trace_fp64_v(const KParams& kp, int blocks, size_t smem, cudaStream_t stream) {
-    cudaFuncSetAttribute(trace_fp64<I, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    trace_fp64<I, B><<<blocks, 128, smem, stream>>>(kp);
+    if (kp.ngroups > 0) {
+        cudaFuncSetAttribute(trace_fp64<I, B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        trace_fp64<I, B, true><<<blocks, 128, smem, stream>>>(kp);
+    } else {
+        cudaFuncSetAttribute(trace_fp64<I, B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        trace_fp64<I, B, false><<<blocks, 128, smem, stream>>>(kp);
+    }
     return cudaGetLastError();
 }
 

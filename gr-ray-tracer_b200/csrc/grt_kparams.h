@@ -98,7 +98,14 @@ struct KParams {
     const KImage* images;
     const unsigned long long* image_start;  // [nimages + 1]
     int nimages;
-    int pad_images;
+    // Channel groups (batched launch, scattering off): images with the same
+    // camera and screen share one geodesic per pixel; queue index q in group g
+    // is pixel q - group_qstart[g] of the images chan_img[group_chan[g] ..
+    // group_chan[g + 1]) (the first is the group's lead).  0 = no sharing.
+    int ngroups;
+    const unsigned long long* group_qstart;  // [ngroups + 1]
+    const int* group_chan;                  // [ngroups + 1]
+    const int* chan_img;                    // [channels]
     KGrid grid;
     KPhotons ph;
     uint64_t n;                // photons in the queue

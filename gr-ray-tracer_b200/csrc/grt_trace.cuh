@@ -73,6 +73,13 @@ struct Lane {
     int mid_call;
     int attempts;
     int img;              // image of a batched launch (0 otherwise)
+    // channel group of a sharing launch: the lane traces the geodesic of
+    // pixel `pix` for every channel image of group `grp`; channel `lead`
+    // lives in registers, the others in their own photon slots
+    int grp, lead, nchan;
+    unsigned done;        // channels already finished (written) on their own
+    int zero_all;         // a shared event zeroed every channel's Stokes vector
+    long long pix;
     int fast;             // precision hint of the current call (mixed form)
     int need_k1;          // the call's k1 = f(state) is still to be evaluated
     double dl_try;
@@ -108,6 +115,48 @@ GRT_DEV void store_photon(const KPhotons& P, const Lane& L, int terminated, doub
     }
     P.terminate[i] = static_cast<uint8_t>(terminated);
     P.phase[i] = static_cast<uint8_t>(L.phase);
+}
+
+// ---- channel groups (frequency channels sharing one geodesic) ----
+GRT_DEV int chan_image(const KParams& kp, int grp, int c) { return kp.chan_img[kp.group_chan[grp] + c]; }
+GRT_DEV long long chan_slot(const KParams& kp, int grp, int c, long long pix) {
+    return static_cast<long long>(kp.image_start[chan_image(kp, grp, c)]) + pix;
+}
+
+// Geodesic part of the photon state of channel slot i (its id, frequency and
+// Stokes vector are its own and already in place).
+GRT_DEV void store_follower(const KPhotons& P, const Lane& L, long long i, int terminated, int phase, double tdisp,
+                            double pdisp, int have_disp, int zero_stokes, double dl) {
+    P.emission_frame_energy[i] = L.emit;
+    P.x0[i] = L.s[0]; P.x1[i] = L.s[1]; P.x2[i] = L.s[2]; P.x3[i] = L.s[3];
+    P.k0[i] = L.s[4]; P.k1[i] = L.s[5]; P.k2[i] = L.s[6]; P.k3[i] = L.s[7];
+    if (zero_stokes) {
+        P.I[i] = 0.0; P.Q[i] = 0.0; P.U[i] = 0.0; P.V[i] = 0.0;
+    }
+    P.dlambda[i] = dl;
+    if (have_disp) {
+        P.theta_disp[i] = tdisp;
+        P.phi_disp[i] = pdisp;
+    }
+    P.terminate[i] = static_cast<uint8_t>(terminated);
+    P.phase[i] = static_cast<uint8_t>(phase);
+}
+
+// Store the lane's photon and, in a sharing launch, every channel still riding
+// on its geodesic.  Returns the number of photons stored.
+template <bool SHARE>
+GRT_DEV int store_all(const KParams& kp, const Lane& L, int terminated, double tdisp, double pdisp, int have_disp) {
+    store_photon(kp.ph, L, terminated, tdisp, pdisp, have_disp);
+    int stored = 1;
+    if (SHARE) {
+        for (int c = 0; c < L.nchan; ++c) {
+            if (c == L.lead || ((L.done >> c) & 1u)) continue;
+            store_follower(kp.ph, L, chan_slot(kp, L.grp, c, L.pix), terminated, L.phase, tdisp, pdisp, have_disp,
+                           L.zero_all, L.dl);
+            ++stored;
+        }
+    }
+    return stored;
 }
 
 // integrate_cart_ks.hpp:142-155.  One right-hand-side site inside a stage
@@ -293,9 +342,23 @@ struct NoRecord {
 // Everything after the integration step of one call (integrate_cart_ks.hpp:307-417).
 // phase0 is the phase loaded at the start of the call.  Returns 1 if the photon
 // terminated.
-template <bool RAW = false, class Rec = NoRecord>
+// Packet generation of photon `id` at `step` (integrate_cart_ks.hpp:325-347).
+GRT_DEV bool generate_packet(const KParams& kp, const FluidSample& fs, uint64_t id, int64_t step, int packets,
+                             double nu_custom, double& nu, double& E) {
+    Philox rng(kp.seed, id, static_cast<uint32_t>(step));
+    if (packets > 0 && kp.generator == 0) return generate_blackbody(fs.fluid, rng, packets, kp.energy, nu, E);
+    if (packets > 0 && kp.generator == 1)
+        return generate_power_law(rng, packets, kp.pl_slope, kp.nu_min, kp.nu_max, kp.energy, nu, E);
+    if (packets > 0) return GeneratePhotonsCustom(fs.fluid, rng, packets, nu_custom, kp.energy, nu, E);
+    return false;
+}
+
+// SHARE: the lane also carries the other channels of its group (their
+// frequencies and Stokes vectors in their photon slots); *ch_term counts the
+// channels that terminated on their own in this call.
+template <bool RAW = false, class Rec = NoRecord, bool SHARE = false>
 GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, double taken, int64_t step,
-                      double& tdisp, double& pdisp, int& have_disp, Rec rec = Rec()) {
+                      double& tdisp, double& pdisp, int& have_disp, Rec rec = Rec(), int* ch_term = nullptr) {
     const KImage& im = image_params(kp, L.img);
     L.radius = ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
     L.have_radius = 1;
@@ -305,17 +368,50 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
     const bool sampled = needs && sample_fluid<RAW>(kp, ax, L.s, L.radius, fs);
     int terminated = 0;
     if (kp.image_mode && backward && sampled) {
-        Philox rng(kp.seed, L.id, static_cast<uint32_t>(step));
         double nu = 0.0, E = 0.0;
-        bool generated = false;
         const double dcode = fs.fluid.density_g_cm3 / kp.density_scale;
         const int packets = ComputeSuperphotonsPerCell(dcode, kp.norm);
-        if (packets > 0 && kp.generator == 0) {
-            generated = generate_blackbody(fs.fluid, rng, packets, kp.energy, nu, E);
-        } else if (packets > 0 && kp.generator == 1) {
-            generated = generate_power_law(rng, packets, kp.pl_slope, kp.nu_min, kp.nu_max, kp.energy, nu, E);
-        } else if (packets > 0) {
-            generated = GeneratePhotonsCustom(fs.fluid, rng, packets, im.nu_custom, kp.energy, nu, E);
+        bool generated = generate_packet(kp, fs, L.id, step, packets, im.nu_custom, nu, E);
+        if (SHARE) {
+            // every other channel draws with its own id and frequency
+            int promote = -1;
+            for (int c = 0; c < L.nchan; ++c) {
+                if (c == L.lead || ((L.done >> c) & 1u)) continue;
+                const long long sc = chan_slot(kp, L.grp, c, L.pix);
+                double nu_c = 0.0, E_c = 0.0;
+                const double f_c = image_params(kp, chan_image(kp, L.grp, c)).nu_custom;
+                if (generate_packet(kp, fs, kp.ph.id[sc], step, packets, f_c, nu_c, E_c)) {
+                    kp.ph.frequency[sc] = nu_c;
+                    kp.ph.I[sc] = E_c;
+                    kp.ph.Q[sc] = 0.0;
+                    kp.ph.U[sc] = 0.0;
+                    kp.ph.V[sc] = 0.0;
+                    if (!generated && promote < 0) promote = c;
+                } else {
+                    // rejected on its own: the state after this step, Stokes zeroed
+                    store_follower(kp.ph, L, sc, 1, 4, 0.0, 0.0, 0, 1, L.dl);
+                    L.done |= 1u << c;
+                    ++*ch_term;
+                }
+            }
+            if (!generated && promote >= 0) {
+                // the lead is rejected on its own; channel `promote` carries on
+                L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+                const int ph_keep = L.phase;
+                L.phase = 4;
+                store_photon(kp.ph, L, 1, 0.0, 0.0, 0);
+                L.phase = ph_keep;
+                L.done |= 1u << L.lead;
+                ++*ch_term;
+                const long long sc = chan_slot(kp, L.grp, promote, L.pix);
+                L.lead = promote;
+                L.idx = sc;
+                L.id = kp.ph.id[sc];
+                L.img = chan_image(kp, L.grp, promote);
+                nu = kp.ph.frequency[sc];
+                E = kp.ph.I[sc];
+                generated = true;
+            }
         }
         if (generated) {
             L.freq = nu;
@@ -349,6 +445,30 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
             if (kp.m_emis) dI = kp.m_emis[fs.cell] * dI;
             L.I[0] += dI;
         }
+        if (SHARE && (kp.abs_on || kp.emis_on)) {
+            for (int c = 0; c < L.nchan; ++c) {
+                if (c == L.lead || ((L.done >> c) & 1u)) continue;
+                const long long sc = chan_slot(kp, L.grp, c, L.pix);
+                const KImage& ic = image_params(kp, chan_image(kp, L.grp, c));
+                const double f_c = kp.ph.frequency[sc];
+                double Ic[4] = {kp.ph.I[sc], kp.ph.Q[sc], kp.ph.U[sc], kp.ph.V[sc]};
+                if (kp.abs_on) {
+                    double dtau = ComputeOpticalDepthIncrement(fs.fluid, f_c, taken, ic.kappa);
+                    if (kp.m_abs) dtau = kp.m_abs[fs.cell] * dtau;
+                    const double att_c = exp(-dtau);
+                    for (int q = 0; q < 4; ++q) Ic[q] *= att_c;
+                }
+                if (kp.emis_on) {
+                    double dI = ComputeEmissivityIncrement(fs.fluid, f_c, taken, ic.jcoef);
+                    if (kp.m_emis) dI = kp.m_emis[fs.cell] * dI;
+                    Ic[0] += dI;
+                }
+                kp.ph.I[sc] = Ic[0];
+                kp.ph.Q[sc] = Ic[1];
+                kp.ph.U[sc] = Ic[2];
+                kp.ph.V[sc] = Ic[3];
+            }
+        }
         if (kp.scat_on) {
             Philox rng(kp.seed, L.id, static_cast<uint32_t>(step));
             ScatterState st;
@@ -374,8 +494,16 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
             const double ee = L.emit;
             if (eo > 0.0 && ee > 0.0 && isfinite(eo) && isfinite(ee)) {
                 L.freq *= eo / ee;
+                if (SHARE) {
+                    for (int c = 0; c < L.nchan; ++c) {
+                        if (c == L.lead || ((L.done >> c) & 1u)) continue;
+                        const long long sc = chan_slot(kp, L.grp, c, L.pix);
+                        kp.ph.frequency[sc] *= eo / ee;
+                    }
+                }
             } else {
                 L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+                L.zero_all = 1;
                 rec.zeroed();
             }
             tdisp = u;
@@ -385,6 +513,7 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
             terminated = 1;
         } else if (crossing < 0) {
             L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+            L.zero_all = 1;
             L.phase = 4;
             terminated = 1;
         }
@@ -392,7 +521,8 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
     return terminated;
 }
 
-template <int INTEGRATOR, class RHS, bool RAW = false>
+// SHARE: queue indices are geodesics of channel groups (KParams::ngroups > 0).
+template <int INTEGRATOR, class RHS, bool RAW = false, bool SHARE = false>
 GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -439,10 +569,26 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                     long long q = -1;
                     if (rank < take_a) q = static_cast<long long>(base_a + rank);
                     else if (rank - take_a < take_b) q = static_cast<long long>(base_b + (rank - take_a));
-                    if (q >= 0 && !kp.ph.terminate[q]) {
-                        load_photon(kp.ph, q, L);
-                        L.idx = q;
-                        L.img = image_of_photon(kp, q);
+                    long long slot = q;
+                    if (SHARE && q >= 0) {
+                        int lo = 0, hi = kp.ngroups - 1;
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (kp.group_qstart[mid] <= static_cast<unsigned long long>(q)) lo = mid;
+                            else hi = mid - 1;
+                        }
+                        L.grp = lo;
+                        L.pix = q - static_cast<long long>(kp.group_qstart[lo]);
+                        L.lead = 0;
+                        L.nchan = kp.group_chan[lo + 1] - kp.group_chan[lo];
+                        L.done = 0;
+                        L.zero_all = 0;
+                        slot = chan_slot(kp, lo, 0, L.pix);
+                    }
+                    if (q >= 0 && !kp.ph.terminate[slot]) {
+                        load_photon(kp.ph, slot, L);
+                        L.idx = slot;
+                        L.img = SHARE ? chan_image(kp, L.grp, 0) : image_of_photon(kp, q);
                         have_disp = 0;
                     }
                 }
@@ -470,6 +616,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                 const double r = L.have_radius ? L.radius : ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
                 if (r <= kp.r_min) {
                     L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+                    L.zero_all = 1;
                     L.phase = 4;
                     finished = terminated = 1;
                 } else if (r > kp.r_max) {
@@ -481,8 +628,14 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                     rk4_step<RHS>(L.s, taken, kp, 1);
                     RHS::after_accept(L.s, kp, 1);
                     ++cnt.accepted;
-                    terminated = post_step<RAW>(kp, ax, L, phase0, taken,
-                                           kp.step0 + L.calls - 1, tdisp, pdisp, have_disp);
+                    int ch_term = 0;
+                    terminated = post_step<RAW, NoRecord, SHARE>(kp, ax, L, phase0, taken, kp.step0 + L.calls - 1,
+                                                                 tdisp, pdisp, have_disp, NoRecord(), &ch_term);
+                    if (SHARE && ch_term) {
+                        cnt.terminated += ch_term;
+                        const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
+                        if (ts > cnt.max_term_step) cnt.max_term_step = ts;
+                    }
                     finished = terminated;
                 } else {
                     // Mixed form: an RK45 call may use the FP32 right-hand side only
@@ -508,8 +661,14 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                 L.dl = L.dl_try;
                 L.mid_call = 0;
                 const int phase0 = L.phase;
-                terminated = post_step<RAW>(kp, ax, L, phase0, taken,
-                                       kp.step0 + L.calls - 1, tdisp, pdisp, have_disp);
+                int ch_term = 0;
+                terminated = post_step<RAW, NoRecord, SHARE>(kp, ax, L, phase0, taken, kp.step0 + L.calls - 1, tdisp,
+                                                             pdisp, have_disp, NoRecord(), &ch_term);
+                if (SHARE && ch_term) {
+                    cnt.terminated += ch_term;
+                    const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
+                    if (ts > cnt.max_term_step) cnt.max_term_step = ts;
+                }
                 finished = terminated;
             } else {
                 ++cnt.rejected;
@@ -521,9 +680,9 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
             }
         }
         if (finished) {
-            store_photon(kp.ph, L, terminated, tdisp, pdisp, have_disp);
+            const int stored = store_all<SHARE>(kp, L, terminated, tdisp, pdisp, have_disp);
             if (terminated) {
-                ++cnt.terminated;
+                cnt.terminated += stored;
                 const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
                 if (ts > cnt.max_term_step) cnt.max_term_step = ts;
             }
@@ -532,7 +691,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
     }
     if (timed_out) {
         // Leave every photon consistent: write back what this lane holds.
-        if (L.idx >= 0) store_photon(kp.ph, L, 0, tdisp, pdisp, have_disp);
+        if (L.idx >= 0) store_all<SHARE>(kp, L, 0, tdisp, pdisp, have_disp);
         if (lane == 0) atomicAdd(&kp.counters->timed_out, 1ull);
     }
     // ---- flush counters: warp reduce, one atomic per counter per warp ----

@@ -83,6 +83,8 @@ def load(path: Path | None = None):
     L.grt_get_batch_image_products.argtypes = [vp, C.c_size_t, P(ImageProducts)]
     L.grt_write_batch_products_npz.argtypes = [vp, C.c_char_p, C.c_char_p]
     L.grt_render_graph.argtypes = [vp, P(RunStats)]
+    L.grt_set_channel_sharing.argtypes = [vp, C.c_int]
+    L.grt_set_channel_sharing.restype = C.c_int
     L.grt_init_image_rows.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]
     L.grt_init_image_rows.restype = C.c_int
     L.grt_init_disk_photons.argtypes = [vp, C.c_uint64, P(C.c_uint64)]
@@ -241,6 +243,10 @@ class Context:
         arr = (ImageSpec * len(specs))(*specs)
         self._check(self.lib.grt_init_image_batch(self._h, arr, len(specs), id_offset))
         self._specs = list(specs)
+
+    def set_channel_sharing(self, enable: bool):
+        """Frequency channels of a batch share their geodesics (default on)."""
+        self._check(self.lib.grt_set_channel_sharing(self._h, int(bool(enable))))
 
     @property
     def batch_image_count(self) -> int:

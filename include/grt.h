@@ -318,6 +318,17 @@ typedef struct grt_image_spec {
 grt_status grt_init_image_batch(grt_ctx* ctx, const grt_image_spec* specs, size_t nimages, uint64_t id_offset);
 size_t grt_batch_image_count(const grt_ctx* ctx);
 
+/*
+ * Frequency channels: images of a batch with identical camera and screen
+ * (theta, phi, distance, width, height, nx, ny) differ only in frequency and
+ * coefficients, which change Stokes vectors but never a geodesic.  With
+ * scattering off they share one traced geodesic per pixel (up to 32 channels
+ * per group); each channel keeps its own id, random draws, frequency and
+ * Stokes vector, and its photons end bit for bit as if traced alone.  On by
+ * default; enable = 0 traces every image separately.
+ */
+grt_status grt_set_channel_sharing(grt_ctx* ctx, int enable);
+
 /* Products of image k of the batch (buffers sized nx_k*ny_k and p.spectrum_bins). */
 grt_status grt_get_batch_image_products(grt_ctx* ctx, size_t image, grt_image_products* out);
 

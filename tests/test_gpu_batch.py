@@ -176,3 +176,48 @@ def test_mixed_precision_batch_error(gpu):
         assert ref[k].image_I.any()
         err = stokes_l2_rel(got[k].image_I, ref[k].image_I)
         assert err <= 1e-5, (k, err)
+
+
+def channel_specs(p):
+    # four frequency channels of one camera, plus one image with another camera
+    f = [(230e9, 1.0), (345e9, 1.5), (86e9, 86.0 / 230.0), (43e9, 43.0 / 230.0)]
+    specs = [abi.ImageSpec.from_params(p, 16, 16, camera_theta=math.radians(17.0), custom_frequency_hz=nu,
+                                       emission_coefficient=j, absorption_coefficient=0.5 * j) for nu, j in f]
+    specs.insert(2, abi.ImageSpec.from_params(p, 12, 12, camera_theta=math.radians(40.0)))
+    return specs
+
+
+@pytest.mark.parametrize("generator", [abi.GEN_CUSTOM, abi.GEN_BLACKBODY])
+def test_channel_sharing_equals_single_images(gpu, oracle, generator):
+    # The four channels share one geodesic per pixel; every channel must end
+    # exactly as if traced alone (own id, draws, frequency and Stokes vector).
+    w = mini(workloads.C2, 16, (32, 16, 16), generator=generator, temperature_k_per_code=1e10)
+    p = w.params()
+    grid = w.torus()
+    specs = channel_specs(p)
+    shared, sprods, sst = run_batch(gpu, p, grid, specs)
+    ctx = gpu.Context(p)
+    try:
+        ctx.set_channel_sharing(False)
+        ctx.upload_grid(grid)
+        ctx.init_image_batch(specs)
+        ust = ctx.run()
+        unshared = ctx.download_photons()
+    finally:
+        ctx.close()
+    for f in abi.PHOTON_FIELDS:
+        assert np.array_equal(getattr(shared, f), getattr(unshared, f)), f
+    n_shared_geodesics = 16 * 16 + 12 * 12
+    assert sst["n_terminated"] == ust["n_terminated"] == shared.n
+    assert sst["photon_calls"] < ust["photon_calls"]  # one geodesic per pixel for the four channels
+    start = 0
+    for k, sp in enumerate(specs):
+        n = sp.nx * sp.ny
+        q = single_params(p, sp)
+        init = oracle.init_image_photons(q, sp.nx, sp.ny, id_offset=start)
+        want, wprod, _ = run_oracle(oracle, q, grid, photons=init)
+        got = abi.PhotonArrays.from_dict({f: getattr(shared, f)[start:start + n] for f in abi.PHOTON_FIELDS})
+        assert_photons_match(got, want)
+        assert_products_match(sprods[k], wprod)
+        start += n
+    assert n_shared_geodesics < shared.n
