@@ -38,7 +38,6 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
 import tempfile
 import time
@@ -70,53 +69,82 @@ def algorithmic_flops(stats, integrator):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock, power and clock-event (throttle) reasons of this rank's GPU,
+    sampled through NVML every 10 ms by a background thread while the timed
+    regions run (nvidia-smi's 200 ms loop would see only a sample or two of a
+    sub-second region)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, device_index):
+    def __init__(self, device_index, period_s=0.010):
         self.dev = device_index
-        self.proc = None
-        self.path = None
+        self.period = period_s
+        self.rows = []
+        self.handle = None
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+        self._active = None
+
+    def _open(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.dev)
+        try:
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+        self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+
+    def _loop(self):
+        import pynvml
+        while not self._stop.is_set():
+            if not self._active.is_set():
+                self._active.wait(0.05)
+                continue
+            try:
+                sm = pynvml.nvmlDeviceGetClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+                reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                power = pynvml.nvmlDeviceGetPowerUsage(self.handle) / 1000.0
+                self.rows.append((sm, reasons, power))
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            self._open()
+        except Exception as e:  # no NVML: report the clocks as unsampled
+            log(f"clock sampler unavailable: {e}")
+            return self
+        self._stop = threading.Event()
+        self._active = threading.Event()
+        self._thread = threading.Thread(target=self._loop, daemon=True)
+        self._thread.start()
         return self
 
+    def timed(self, on):
+        """Sample only while a timed region runs."""
+        if self._active is not None:
+            (self._active.set if on else self._active.clear)()
+
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        if self._thread:
+            self._stop.set()
+            self._thread.join(timeout=5)
 
     def summary(self):
-        rows = []
-        try:
-            for line in open(self.path):
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        except OSError:
-            pass
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "samples": 0}
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({name for _, bits, _ in self.rows for name, bit in self.REASONS if bits & bit})
+        return {"sm_mhz": statistics.median(sm), "sm_min_mhz": min(sm), "sm_max_mhz": self.max_mhz,
+                "power_w_max": max(r[2] for r in self.rows), "reasons": reasons, "samples": len(self.rows),
+                "source": f"NVML every {self.period * 1e3:.0f} ms during the timed regions"}
 
 
 def dist_setup(n_gpus):
@@ -260,44 +288,45 @@ def run_ours(args):
 
     results = {}
     images = {}
-    sampler = ClockSampler(local)
-    with sampler:
-        for name, (ctx, batched) in forms.items():
-            prepare(ctx, batched)
-            for _ in range(args.warmup):
-                one_step(ctx, batched)
-            torch.cuda.synchronize()
-            barrier(world)
-            total_ms = 0.0
-            trace_ms = 0.0
-            launches = 0
-            stats_acc = None
-            for _ in range(args.steps):
-                with torch.cuda.stream(stream):
-                    flush_buf.zero_()
-                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                ev0.record(stream)
-                st, prod = one_step(ctx, batched)
-                ev1.record(stream)
-                ev1.synchronize()
-                total_ms += ev0.elapsed_time(ev1)
-                trace_ms += st["trace_ms"]
-                # our kernels per step: inits + trace launches + products
-                launches += (len(specs) if batched else 1) * 2 + st["launches"]
-                stats_acc = st
-            torch.cuda.synchronize()
-            barrier(world)
-            total_ms = max_over_ranks(total_ms, world)
-            n_rays = bw.rays if batched else w.pixels * w.pixels
-            if batched:
-                images[name] = [ctx.batch_image_products(k).image_I.copy() for k in range(len(specs))]
-            else:
-                images[name] = [prod.image_I.copy()]
-            results[name] = dict(ms_per_step=total_ms / args.steps, trace_ms_per_launch=trace_ms / args.steps,
-                                 stats=stats_acc, launches=launches, rays=n_rays,
-                                 rays_per_s=world * n_rays * args.steps / (total_ms * 1e-3),
-                                 rk_steps_per_s=world * stats_acc["accepted_steps"] * args.steps / (total_ms * 1e-3))
-    clocks = sampler.summary()
+    sampler = ClockSampler(local).__enter__()
+    for name, (ctx, batched) in forms.items():
+        prepare(ctx, batched)
+        for _ in range(args.warmup):
+            one_step(ctx, batched)
+        torch.cuda.synchronize()
+        barrier(world)
+        total_ms = 0.0
+        trace_ms = 0.0
+        launches = 0
+        stats_acc = None
+        sampler.timed(True)
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush_buf.zero_()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            st, prod = one_step(ctx, batched)
+            ev1.record(stream)
+            ev1.synchronize()
+            total_ms += ev0.elapsed_time(ev1)
+            trace_ms += st["trace_ms"]
+            # our kernels per step: one init per image, the trace launches and
+            # the products launches (up to 32 images each)
+            launches += (len(specs) + -(-len(specs) // 32) if batched else 2) + st["launches"]
+            stats_acc = st
+        sampler.timed(False)
+        torch.cuda.synchronize()
+        barrier(world)
+        total_ms = max_over_ranks(total_ms, world)
+        n_rays = bw.rays if batched else w.pixels * w.pixels
+        if batched:
+            images[name] = [ctx.batch_image_products(k).image_I.copy() for k in range(len(specs))]
+        else:
+            images[name] = [prod.image_I.copy()]
+        results[name] = dict(ms_per_step=total_ms / args.steps, trace_ms_per_launch=trace_ms / args.steps,
+                             stats=stats_acc, launches=launches, rays=n_rays,
+                             rays_per_s=world * n_rays * args.steps / (total_ms * 1e-3),
+                             rk_steps_per_s=world * stats_acc["accepted_steps"] * args.steps / (total_ms * 1e-3))
 
     # Stokes-I error of every frequency channel of the mixed batch against the
     # FP64 image of the same channel (the FP64 batch is bitwise the FP64 form
@@ -356,6 +385,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier(world)
     e2e_ms = 0.0
+    sampler.timed(True)
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush_buf.zero_()
@@ -365,6 +395,9 @@ def run_ours(args):
         ev1.record(stream)
         ev1.synchronize()
         e2e_ms += ev0.elapsed_time(ev1)
+    sampler.timed(False)
+    sampler.__exit__(None, None, None)
+    clocks = sampler.summary()
     e2e_ms = max_over_ranks(e2e_ms, world)
     p = ctx.params
     d2h = sum(8 * (4 * o.nx * o.ny + p.spectrum_bins + 1) for o in host_out)

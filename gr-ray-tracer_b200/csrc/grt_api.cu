@@ -776,36 +776,53 @@ grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages
     return launch_image_inits(c);
 }
 
-// build_observation_products (observation.hpp:31-84) for photon slots
-// [offset, offset + n) into device buffers.
+// Launch-wide part of a build_observation_products (observation.hpp:31-84) launch.
+grt::ProductsSet products_set(grt_ctx* c) {
+    const grt_params& p = c->p;
+    grt::ProductsSet set;
+    std::memset(&set, 0, sizeof(set));
+    set.ph = c->ph.view();
+    set.bins = p.spectrum_bins;
+    set.spec_min = p.spectrum_min_hz;
+    set.spec_max = p.spectrum_max_hz;
+    set.log_min = std::log10(p.spectrum_min_hz);
+    set.log_max = std::log10(p.spectrum_max_hz);
+    return set;
+}
+
+grt::ProductsImage products_image(unsigned long long offset, unsigned long long n, uint64_t nx, uint64_t ny, double W,
+                                  double H, double* image, double* spectrum, unsigned long long* arrived) {
+    grt::ProductsImage im;
+    std::memset(&im, 0, sizeof(im));
+    im.offset = offset;
+    im.n = n;
+    im.nx = nx;
+    im.ny = ny;
+    im.W = W;
+    im.H = H;
+    im.image = image;
+    im.spectrum = spectrum;
+    im.arrived = arrived;
+    return im;
+}
+
+// Products of photon slots [offset, offset + n) as one image into device buffers.
 grt_status launch_products(grt_ctx* c, unsigned long long offset, unsigned long long n, uint64_t nx, uint64_t ny,
                            double W, double H, double* image, double* spectrum, unsigned long long* arrived) {
-    const grt_params& p = c->p;
-    const size_t npix = nx * ny, bins = p.spectrum_bins;
+    const size_t npix = nx * ny, bins = c->p.spectrum_bins;
     GRT_CUDA(c, cudaMemsetAsync(image, 0, 4 * npix * sizeof(double), c->stream), "memset");
-    GRT_CUDA(c, cudaMemsetAsync(spectrum, 0, bins * sizeof(double), c->stream), "memset");
+    if (bins) GRT_CUDA(c, cudaMemsetAsync(spectrum, 0, bins * sizeof(double), c->stream), "memset");
     GRT_CUDA(c, cudaMemsetAsync(arrived, 0, sizeof(unsigned long long), c->stream), "memset");
-    grt::ProductsArgs a;
-    a.ph = c->ph.view();
-    a.offset = offset;
-    a.n = n;
-    a.nx = nx;
-    a.ny = ny;
-    a.bins = bins;
-    a.W = W;
-    a.H = H;
-    a.spec_min = p.spectrum_min_hz;
-    a.spec_max = p.spectrum_max_hz;
-    a.log_min = std::log10(p.spectrum_min_hz);
-    a.log_max = std::log10(p.spectrum_max_hz);
-    a.image = image;
-    a.spectrum = spectrum;
-    a.arrived = arrived;
-    GRT_CUDA(c, grt::launch_image_products(a, c->stream), "image_products");
+    grt::ProductsSet set = products_set(c);
+    set.nimages = 1;
+    set.img[0] = products_image(offset, n, nx, ny, W, H, image, spectrum, arrived);
+    GRT_CUDA(c, grt::launch_image_products(set, c->stream), "image_products");
     return GRT_OK;
 }
 
-// Products of every image of the image set into the per-image device buffers.
+// Products of every image of the image set into the per-image device buffers
+// (contiguous, so three memsets clear them all), kProductsMaxImages images
+// per launch.
 grt_status launch_all_products(grt_ctx* c) {
     const size_t nimg = c->images.size(), bins = c->p.spectrum_bins;
     c->bimage_off.assign(nimg + 1, 0);
@@ -813,12 +830,22 @@ grt_status launch_all_products(grt_ctx* c) {
     GRT_CUDA(c, c->bimage.alloc(c->bimage_off[nimg]), "alloc products");
     GRT_CUDA(c, c->bspectrum.alloc(nimg * bins), "alloc products");
     GRT_CUDA(c, c->barrived.alloc(nimg), "alloc products");
-    for (size_t k = 0; k < nimg; ++k) {
-        const grt_image_spec& sp = c->images[k];
-        grt_status st = launch_products(c, c->image_start[k], c->image_start[k + 1] - c->image_start[k], sp.nx, sp.ny,
-                                        sp.camera_width, sp.camera_height, c->bimage.ptr + c->bimage_off[k],
-                                        c->bspectrum.ptr + k * bins, c->barrived.ptr + k);
-        if (st != GRT_OK) return st;
+    if (nimg == 0) return GRT_OK;
+    GRT_CUDA(c, cudaMemsetAsync(c->bimage.ptr, 0, c->bimage_off[nimg] * sizeof(double), c->stream), "memset");
+    if (bins) GRT_CUDA(c, cudaMemsetAsync(c->bspectrum.ptr, 0, nimg * bins * sizeof(double), c->stream), "memset");
+    GRT_CUDA(c, cudaMemsetAsync(c->barrived.ptr, 0, nimg * sizeof(unsigned long long), c->stream), "memset");
+    for (size_t k0 = 0; k0 < nimg; k0 += grt::kProductsMaxImages) {
+        grt::ProductsSet set = products_set(c);
+        const size_t k1 = std::min(nimg, k0 + static_cast<size_t>(grt::kProductsMaxImages));
+        for (size_t k = k0; k < k1; ++k) {
+            const grt_image_spec& sp = c->images[k];
+            set.img[k - k0] = products_image(c->image_start[k], c->image_start[k + 1] - c->image_start[k], sp.nx,
+                                             sp.ny, sp.camera_width, sp.camera_height,
+                                             c->bimage.ptr + c->bimage_off[k], c->bspectrum.ptr + k * bins,
+                                             c->barrived.ptr + k);
+        }
+        set.nimages = static_cast<int>(k1 - k0);
+        GRT_CUDA(c, grt::launch_image_products(set, c->stream), "image_products");
     }
     return GRT_OK;
 }

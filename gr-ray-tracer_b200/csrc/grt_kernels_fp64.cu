@@ -60,31 +60,53 @@ __global__ void init_image_pixels(const __grid_constant__ InitImageArgs args) {
 }
 
 
-// observation.hpp:61-82: ImageArrived photons binned by arrival (u, v) and log10(nu).
-__global__ void image_products(const __grid_constant__ ProductsArgs args) {
-    const unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
-    bool arrived = false;
-    if (i < args.n) {
-        const unsigned long long o = args.offset + i;
-        if (args.ph.phase[o] == 3) {
-            arrived = true;
-            const unsigned long long px = dev::observation_bin(args.ph.theta_disp[o], -0.5 * args.W, 0.5 * args.W, args.nx);
-            const unsigned long long py = dev::observation_bin(args.ph.phi_disp[o], -0.5 * args.H, 0.5 * args.H, args.ny);
-            const unsigned long long pix = py * args.nx + px;
-            const double I = args.ph.I[o];
-            atomicAdd(&args.image[pix], I);
-            atomicAdd(&args.image[args.nx * args.ny + pix], args.ph.Q[o]);
-            atomicAdd(&args.image[2 * args.nx * args.ny + pix], args.ph.U[o]);
-            atomicAdd(&args.image[3 * args.nx * args.ny + pix], args.ph.V[o]);
-            const double f = args.ph.frequency[o];
-            if (f >= args.spec_min && f <= args.spec_max) {
-                const unsigned long long b = dev::observation_bin(log10(f), args.log_min, args.log_max, args.bins);
-                atomicAdd(&args.spectrum[b], I);
-            }
+// observation.hpp:61-82: ImageArrived photons binned by arrival (u, v) and
+// log10(nu).  Each block serves one image of the set; its spectrum is summed
+// in shared memory first (the arrival frequencies of an image crowd into a few
+// bins, so per-photon global atomics would serialise on them) and flushed with
+// one global atomic per non-empty bin.
+__global__ void __launch_bounds__(256) image_products(const __grid_constant__ ProductsSet set) {
+    extern __shared__ double hist[];
+    __shared__ unsigned long long s_arrived;
+    int k = 0;
+    while (k + 1 < set.nimages && set.img[k + 1].block0 <= blockIdx.x) ++k;
+    const ProductsImage& im = set.img[k];
+    const unsigned end = k + 1 < set.nimages ? set.img[k + 1].block0 : set.blocks;
+    const unsigned long long stride = static_cast<unsigned long long>(end - im.block0) * blockDim.x;
+    const bool shared_spec = set.bins <= kProductsSharedBins;
+    if (shared_spec)
+        for (unsigned long long q = threadIdx.x; q < set.bins; q += blockDim.x) hist[q] = 0.0;
+    if (threadIdx.x == 0) s_arrived = 0;
+    __syncthreads();
+    const unsigned long long npix = im.nx * im.ny;
+    unsigned long long count = 0;
+    for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x - im.block0) * blockDim.x + threadIdx.x;
+         i < im.n; i += stride) {
+        const unsigned long long o = im.offset + i;
+        if (set.ph.phase[o] != 3) continue;
+        ++count;
+        const unsigned long long px = dev::observation_bin(set.ph.theta_disp[o], -0.5 * im.W, 0.5 * im.W, im.nx);
+        const unsigned long long py = dev::observation_bin(set.ph.phi_disp[o], -0.5 * im.H, 0.5 * im.H, im.ny);
+        const unsigned long long pix = py * im.nx + px;
+        const double I = set.ph.I[o];
+        atomicAdd(&im.image[pix], I);
+        atomicAdd(&im.image[npix + pix], set.ph.Q[o]);
+        atomicAdd(&im.image[2 * npix + pix], set.ph.U[o]);
+        atomicAdd(&im.image[3 * npix + pix], set.ph.V[o]);
+        const double f = set.ph.frequency[o];
+        if (set.bins > 0 && f >= set.spec_min && f <= set.spec_max) {
+            const unsigned long long b = dev::observation_bin(log10(f), set.log_min, set.log_max, set.bins);
+            atomicAdd(shared_spec ? &hist[b] : &im.spectrum[b], I);
         }
     }
-    const unsigned mask = __ballot_sync(0xFFFFFFFFu, arrived);
-    if ((threadIdx.x & 31) == 0 && mask) atomicAdd(args.arrived, static_cast<unsigned long long>(__popc(mask)));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) count += __shfl_down_sync(0xFFFFFFFFu, count, off);
+    if ((threadIdx.x & 31) == 0 && count) atomicAdd(&s_arrived, count);
+    __syncthreads();
+    if (shared_spec)
+        for (unsigned long long q = threadIdx.x; q < set.bins; q += blockDim.x)
+            if (hist[q] != 0.0) atomicAdd(&im.spectrum[q], hist[q]);
+    if (threadIdx.x == 0 && s_arrived) atomicAdd(im.arrived, s_arrived);
 }
 
 __global__ void count_terminated(const uint8_t* __restrict__ term, unsigned long long n,
@@ -237,11 +259,19 @@ cudaError_t launch_init_disk(const DiskInitArgs& a, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_image_products(const ProductsArgs& args, cudaStream_t stream) {
-    if (args.n == 0) return cudaSuccess;
+cudaError_t launch_image_products(ProductsSet& set, cudaStream_t stream) {
     const unsigned threads = 256;
-    const unsigned blocks = static_cast<unsigned>((args.n + threads - 1) / threads);
-    image_products<<<blocks, threads, 0, stream>>>(args);
+    unsigned long long blocks = 0;
+    for (int k = 0; k < set.nimages; ++k) {
+        set.img[k].block0 = static_cast<unsigned>(blocks);
+        // about four arrivals per thread: few blocks, so few spectrum flushes
+        blocks += (set.img[k].n + 4 * threads - 1) / (4 * threads);
+    }
+    if (blocks == 0) return cudaSuccess;
+    if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
+    set.blocks = static_cast<unsigned>(blocks);
+    const size_t smem = set.bins <= kProductsSharedBins ? set.bins * sizeof(double) : 0;
+    image_products<<<set.blocks, threads, smem, stream>>>(set);
     return cudaGetLastError();
 }
 

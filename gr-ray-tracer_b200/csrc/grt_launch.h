@@ -50,15 +50,29 @@ struct DiskInitArgs {
     double dlambda0;                     // initial_step (disk mode: unscaled)
 };
 
-struct ProductsArgs {
-    KPhotons ph;
+// One image of a products launch: its photon slots, screen and output buffers.
+struct ProductsImage {
     unsigned long long offset, n;  // photon slots [offset, offset + n)
-    unsigned long long nx, ny, bins;
+    unsigned long long nx, ny;
     double W, H;
+    double* image;                 // [4][ny][nx] (I, Q, U, V), zeroed before the launch
+    double* spectrum;              // [bins], zeroed
+    unsigned long long* arrived;   // [1], zeroed
+    unsigned block0;               // first block of this image in the launch
+    unsigned pad;
+};
+
+// build_observation_products over up to kProductsMaxImages images in one
+// launch; each block belongs to one image.
+constexpr int kProductsMaxImages = 32;
+constexpr unsigned long long kProductsSharedBins = 4096;  // spectrum privatised in shared memory up to this
+struct ProductsSet {
+    KPhotons ph;
+    unsigned long long bins;
     double spec_min, spec_max, log_min, log_max;
-    double* image;                 // [4][ny][nx] (I, Q, U, V)
-    double* spectrum;              // [bins]
-    unsigned long long* arrived;   // [1]
+    int nimages;
+    unsigned blocks;
+    ProductsImage img[kProductsMaxImages];
 };
 
 // Buffers of the adjoint pass (grt_adjoint.cu).
@@ -122,7 +136,8 @@ cudaError_t launch_trace_mixed(const KParams& kp, int integrator, int sm_count, 
                                cudaStream_t stream);
 cudaError_t launch_init_image(const InitImageArgs& args, cudaStream_t stream);
 cudaError_t launch_init_disk(const DiskInitArgs& a, cudaStream_t stream);
-cudaError_t launch_image_products(const ProductsArgs& args, cudaStream_t stream);
+// Fills block0 / blocks of `set` and launches it.
+cudaError_t launch_image_products(ProductsSet& set, cudaStream_t stream);
 cudaError_t launch_count_terminated(const uint8_t* term, unsigned long long n, unsigned long long* out,
                                     int sm_count, cudaStream_t stream);
 
