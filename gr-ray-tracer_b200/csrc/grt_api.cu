@@ -119,7 +119,7 @@ struct grt_ctx {
     DevBuf<unsigned long long> arrived;
     DevBuf<unsigned long long> scratch_u64;
     unsigned long long* host_u64 = nullptr;  // pinned
-    grt_launch_config lc{128, 4, 1, 32};
+    grt_launch_config lc{128, 4, 1, 32, 1};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // images of the last grt_init_image_photons (one, cameras from p) or
     // grt_init_image_batch call; image k owns photon slots
@@ -141,6 +141,8 @@ struct grt_ctx {
     unsigned long long geodesics = 0;     // queue length with sharing
     DevBuf<unsigned long long> group_qstart_dev;
     DevBuf<int> group_chan_dev, chan_img_dev;
+    DevBuf<unsigned long long> share_state;  // [geodesics] lead / finished channels (KParams::share_state)
+    DevBuf<long long> calls_carry;           // [queue] calls taken in the backward-leg launch
     // per-image products of a batch: image k's I,Q,U,V at bimage + bimage_off[k]
     DevBuf<double> bimage, bspectrum;
     DevBuf<unsigned long long> barrived;
@@ -311,7 +313,9 @@ grt::KParams make_kparams(const grt_ctx* c) {
         k.group_chan = c->group_chan_dev.ptr;
         k.chan_img = c->chan_img_dev.ptr;
         k.n = c->geodesics;
+        k.share_state = c->share_state.ptr;
     }
+    k.calls_carry = c->calls_carry.ptr;
     k.counters = c->counters.ptr;
     k.refill_threshold = c->lc.refill_threshold;
     k.grab = c->lc.photons_per_grab;
@@ -428,6 +432,7 @@ grt_status grt_set_launch_config(grt_ctx* c, const grt_launch_config* cfg) {
         return fail(c, GRT_EINVAL, "refill_threshold must be in [1, 32]");
     if (cfg->photons_per_grab < 1 || cfg->photons_per_grab > (1 << 20))
         return fail(c, GRT_EINVAL, "photons_per_grab must be in [1, 2^20]");
+    if (cfg->split_legs != 0 && cfg->split_legs != 1) return fail(c, GRT_EINVAL, "split_legs must be 0 or 1");
     c->lc = *cfg;
     ++c->generation;
     return GRT_OK;
@@ -602,6 +607,9 @@ grt_status grt_upload_photons(grt_ctx* c, const grt_photon_soa* s, size_t n) {
         GRT_CUDA(c, cudaMemcpyAsync(c->ph.f[q].ptr, src[q], n * 8, cudaMemcpyHostToDevice, c->stream), "H2D photons");
     GRT_CUDA(c, cudaMemcpyAsync(c->ph.term.ptr, s->terminate, n, cudaMemcpyHostToDevice, c->stream), "H2D term");
     GRT_CUDA(c, cudaMemcpyAsync(c->ph.phase.ptr, s->phase, n, cudaMemcpyHostToDevice, c->stream), "H2D phase");
+    if (keep_images && c->batched && c->groups_share && c->geodesics)
+        GRT_CUDA(c, cudaMemsetAsync(c->share_state.ptr, 0, c->geodesics * sizeof(unsigned long long), c->stream),
+                 "memset share state");
     return count_initial_terminated(c);
 }
 
@@ -645,6 +653,10 @@ grt_image_spec spec_from_params(const grt_params& p, uint64_t nx, uint64_t ny) {
 // the context's image set, pixel-centre screen points.
 grt_status launch_image_inits(grt_ctx* c) {
     const grt_params& p = c->p;
+    // fresh rays: channel 0 leads every shared geodesic and none has finished
+    if (c->batched && c->groups_share && c->geodesics)
+        GRT_CUDA(c, cudaMemsetAsync(c->share_state.ptr, 0, c->geodesics * sizeof(unsigned long long), c->stream),
+                 "memset share state");
     for (size_t k = 0; k < c->images.size(); ++k) {
         const grt_image_spec& sp = c->images[k];
         grt::InitImageArgs a;
@@ -760,6 +772,7 @@ grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages
         }
         c->ngroups = static_cast<int>(groups.size());
         c->geodesics = qstart.back();
+        if (c->groups_share) GRT_CUDA(c, c->share_state.alloc(c->geodesics), "alloc share state");
         GRT_CUDA(c, c->group_qstart_dev.alloc(qstart.size()), "alloc groups");
         GRT_CUDA(c, c->group_chan_dev.alloc(gchan.size()), "alloc groups");
         GRT_CUDA(c, c->chan_img_dev.alloc(chan.size()), "alloc groups");
@@ -869,11 +882,32 @@ unsigned long long iteration_limit(const grt::KParams& kp, unsigned long long to
            (1ull << 20);
 }
 
+// Image-mode rays are traced by two launches, the backward leg then the rest
+// (trace_body LEG 1 and 2), unless the launch shape asks for one.
+bool split_legs(const grt_ctx* c) { return c->lc.split_legs != 0 && c->p.mode == GRT_MODE_IMAGE; }
+
+// Device buffers a trace needs besides the photons; allocated before any
+// launch or graph capture.
+grt_status prepare_trace_buffers(grt_ctx* c, unsigned long long queue) {
+    if (split_legs(c)) GRT_CUDA(c, c->calls_carry.alloc(queue), "alloc call carry");
+    return GRT_OK;
+}
+
+// The trace of one chunk of the step loop: one launch over whole rays, or the
+// backward-leg launch and then, with the queue head reset, the forward-leg
+// launch over the same queue.
 cudaError_t launch_trace(const grt_ctx* c, const grt::KParams& kp, size_t smem) {
     const grt_params& p = c->p;
-    return p.precision == GRT_PREC_MIXED
-               ? grt::launch_trace_mixed(kp, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream)
-               : grt::launch_trace_fp64(kp, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+    const bool mixed = p.precision == GRT_PREC_MIXED;
+    if (!split_legs(c))
+        return grt::launch_trace(kp, mixed, 0, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+    cudaError_t e = cudaMemsetAsync(kp.calls_carry, 0, kp.n * sizeof(long long), c->stream);
+    if (e == cudaSuccess)
+        e = grt::launch_trace(kp, mixed, 1, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&kp.counters->queue_head, 0, sizeof(unsigned long long), c->stream);
+    if (e == cudaSuccess)
+        e = grt::launch_trace(kp, mixed, 2, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+    return e;
 }
 
 size_t trace_smem(const grt_ctx* c) {
@@ -1051,6 +1085,11 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
         return GRT_OK;
     }
     grt::KParams kp = make_kparams(c);
+    {
+        const grt_status bs = prepare_trace_buffers(c, kp.n);
+        if (bs != GRT_OK) return bs;
+        kp.calls_carry = c->calls_carry.ptr;
+    }
     const int threads = 128;
     const size_t smem = trace_smem(c);
     const int blocks = c->sm_count * c->lc.blocks_per_sm;
@@ -1096,7 +1135,7 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
         st.accepted_steps += k.accepted;
         st.rejected_attempts += k.rejected;
         st.photon_calls += k.calls;
-        st.launches += 1;
+        st.launches += split_legs(c) ? 2 : 1;
         if (k.max_term_step > max_term_step) max_term_step = k.max_term_step;
         if (k.timed_out) {
             st.timed_out = 1;
@@ -1138,6 +1177,11 @@ grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
         GRT_CUDA(c, c->bspectrum.alloc(nimg * bins), "alloc products");
         GRT_CUDA(c, c->barrived.alloc(nimg), "alloc products");
         grt::KParams kp = make_kparams(c);
+        {
+            const grt_status bs = prepare_trace_buffers(c, kp.n);
+            if (bs != GRT_OK) return bs;
+            kp.calls_carry = c->calls_carry.ptr;
+        }
         kp.step0 = 0;
         kp.budget = p.max_steps;
         kp.max_iterations = iteration_limit(kp, c->n, c->sm_count * c->lc.blocks_per_sm, 128);
@@ -1181,7 +1225,7 @@ grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
     st.accepted_steps = k.accepted;
     st.rejected_attempts = k.rejected;
     st.photon_calls = k.calls;
-    st.launches = 1;
+    st.launches = split_legs(c) ? 2 : 1;
     st.n_terminated = k.terminated;
     st.trace_ms = ms;
     st.steps_done = single_launch_steps_done(p, k.terminated, c->n, k.max_term_step);

@@ -1,26 +1,16 @@
-// FP64 parity-form kernels.  Built with -fmad=false so that every product and
-// sum rounds separately, as in the reference's host build.
+// FP64 kernels around the trace, built with -fmad=false so that every product
+// and sum rounds separately, as in the reference's host build:
 //
-//   trace_fp64<RK4|RK45>  -- persistent per-photon step loop (integrate_cart_ks.hpp:230-419)
 //   init_image_pixels     -- pixel-grid camera rays (initialize_photons.hpp:82-170)
 //   image_products        -- build_observation_products (observation.hpp:31-84)
 //   init_disk_photons     -- initialize_photons_disk (initialize_photons.hpp:173-327)
 //   count_terminated      -- "Count Terminated Photons" (integrate_cart_ks.hpp:496-503)
+//
+// and the dispatcher over the trace kernels of grt_trace_inst.cu.
 #include "grt_launch.h"
 #include "grt_trace.cuh"
 
 namespace grt {
-
-// 128-thread blocks; MINB resident blocks per SM caps the registers per
-// thread at 65536 / (128 * MINB): 255, 170 and 128 for MINB = 2, 3, 4.
-template <int INTEGRATOR, int MINB, bool SHARE>
-__global__ void __launch_bounds__(128, MINB) trace_fp64(const __grid_constant__ KParams kp) {
-    extern __shared__ double smem[];
-    dev::Axes ax;
-    dev::KStore kk;
-    dev::stage_grid(kp, smem, INTEGRATOR, ax, kk);
-    dev::trace_body<INTEGRATOR, dev::Fp64Rhs, false, SHARE>(kp, ax, kk);
-}
 
 // initialize_photons.hpp:116-169 with screen (u, v) at pixel centres; the
 // camera centre and basis come from the host (glibc sin/cos, like the reference).
@@ -208,35 +198,16 @@ __global__ void init_disk_photons(const __grid_constant__ DiskInitArgs args) {
 }
 
 // ---- host-side launchers ----
-template <int I, int B>
-static cudaError_t launch_trace_fp64_v(const KParams& kp, int blocks, size_t smem, cudaStream_t stream) {
-    if (kp.ngroups > 0) {
-        cudaFuncSetAttribute(trace_fp64<I, B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        trace_fp64<I, B, true><<<blocks, 128, smem, stream>>>(kp);
-    } else {
-        cudaFuncSetAttribute(trace_fp64<I, B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        trace_fp64<I, B, false><<<blocks, 128, smem, stream>>>(kp);
-    }
-    return cudaGetLastError();
-}
-
-// 128-thread blocks, sm_count * blocks_per_sm of them; blocks_per_sm (2, 3
-// or 4) selects the register-capped instantiation.
-cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int sm_count, int blocks_per_sm, size_t smem,
-                           cudaStream_t stream) {
+cudaError_t launch_trace(const KParams& kp, bool mixed, int leg, int integrator, int sm_count, int blocks_per_sm,
+                         size_t smem, cudaStream_t stream) {
     const int blocks = sm_count * blocks_per_sm;
-    if (integrator == 0) {
-        switch (blocks_per_sm) {
-            case 2: return launch_trace_fp64_v<0, 2>(kp, blocks, smem, stream);
-            case 3: return launch_trace_fp64_v<0, 3>(kp, blocks, smem, stream);
-            case 4: return launch_trace_fp64_v<0, 4>(kp, blocks, smem, stream);
-            default: return cudaErrorInvalidConfiguration;
-        }
-    }
-    switch (blocks_per_sm) {
-        case 2: return launch_trace_fp64_v<1, 2>(kp, blocks, smem, stream);
-        case 3: return launch_trace_fp64_v<1, 3>(kp, blocks, smem, stream);
-        case 4: return launch_trace_fp64_v<1, 4>(kp, blocks, smem, stream);
+    switch (leg + (mixed ? 3 : 0)) {
+        case 0: return launch_trace_fp64_leg0(kp, integrator, blocks_per_sm, blocks, smem, stream);
+        case 1: return launch_trace_fp64_leg1(kp, integrator, blocks_per_sm, blocks, smem, stream);
+        case 2: return launch_trace_fp64_leg2(kp, integrator, blocks_per_sm, blocks, smem, stream);
+        case 3: return launch_trace_mixed_leg0(kp, integrator, blocks_per_sm, blocks, smem, stream);
+        case 4: return launch_trace_mixed_leg1(kp, integrator, blocks_per_sm, blocks, smem, stream);
+        case 5: return launch_trace_mixed_leg2(kp, integrator, blocks_per_sm, blocks, smem, stream);
         default: return cudaErrorInvalidConfiguration;
     }
 }

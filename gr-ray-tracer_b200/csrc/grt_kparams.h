@@ -113,6 +113,13 @@ struct KParams {
     int64_t budget;            // calls each live photon may take in this launch
     unsigned long long max_iterations;  // per-warp loop limit (GRT_ETIMEOUT)
     KCounters* counters;
+    // two-launch image mode (trace_body LEG 1 then 2): calls each photon took
+    // in the backward-leg launch, by queue index, zeroed before it
+    long long* calls_carry;
+    // channel groups: (lead channel << 32) | finished-channel mask of each
+    // geodesic as the last launch left it; zeroed with the photons' init
+    // (nullptr: channel 0 leads and none finished)
+    unsigned long long* share_state;
     int refill_threshold;      // idle lanes before a warp refills (1..32)
     int grab;                  // photons claimed per queue access (per warp)
     const double* m_abs;       // optional per-cell multipliers on dtau (nullptr = 1)

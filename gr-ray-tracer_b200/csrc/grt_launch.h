@@ -128,12 +128,25 @@ cudaError_t launch_adjoint_forward(const KParams& kp, const AdjointArgs& aa, int
 cudaError_t launch_adjoint_reverse(const KParams& kp, const AdjointArgs& aa, int blocks, size_t smem,
                                    cudaStream_t stream);
 
-// Persistent trace launches: sm_count * blocks_per_sm blocks of 128 threads;
-// blocks_per_sm in {2, 3, 4} picks the register cap (255 / 170 / 128).
-cudaError_t launch_trace_fp64(const KParams& kp, int integrator, int sm_count, int blocks_per_sm, size_t smem,
-                              cudaStream_t stream);
-cudaError_t launch_trace_mixed(const KParams& kp, int integrator, int sm_count, int blocks_per_sm, size_t smem,
-                               cudaStream_t stream);
+// Persistent trace launches (grt_trace_inst.cu): `blocks` blocks of 128
+// threads; blocks_per_sm in {2, 3, 4} picks the register cap (255 / 170 /
+// 128); leg 0 traces whole rays, legs 1 and 2 the backward leg and the rest
+// of image-mode rays (trace_body).
+cudaError_t launch_trace_fp64_leg0(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
+                                   cudaStream_t stream);
+cudaError_t launch_trace_fp64_leg1(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
+                                   cudaStream_t stream);
+cudaError_t launch_trace_fp64_leg2(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
+                                   cudaStream_t stream);
+cudaError_t launch_trace_mixed_leg0(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
+                                    cudaStream_t stream);
+cudaError_t launch_trace_mixed_leg1(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
+                                    cudaStream_t stream);
+cudaError_t launch_trace_mixed_leg2(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
+                                    cudaStream_t stream);
+// sm_count * blocks_per_sm blocks of the form's (FP64 or mixed) kernel for `leg`.
+cudaError_t launch_trace(const KParams& kp, bool mixed, int leg, int integrator, int sm_count, int blocks_per_sm,
+                         size_t smem, cudaStream_t stream);
 cudaError_t launch_init_image(const InitImageArgs& args, cudaStream_t stream);
 cudaError_t launch_init_disk(const DiskInitArgs& a, cudaStream_t stream);
 // Fills block0 / blocks of `set` and launches it.

@@ -1,4 +1,4 @@
-// Mixed FP32/FP64 trace kernels.
+// Mixed FP32/FP64 right-hand-side policy of the trace kernels.
 //
 // Right-hand side of Hamilton's equations (kerr_schild_core.hpp:157-192):
 //   * FP32 form (ks_rhs_fp32): the exact flat-space part dx^mu/dlambda =
@@ -6,7 +6,7 @@
 //     and dp/dlambda are evaluated in FP32; being O(M/r) of the flat part,
 //     their FP32 rounding enters the trajectory at ~1e-7 M/r relative;
 //   * otherwise the FP64 parity form (ks_rhs), bit-identical to the plain
-//     kernel (this translation unit is also built with -fmad=false).
+//     kernel (the trace kernels are built with -fmad=false).
 // Which one a call uses: RK4 calls (fixed step) use FP32; an RK45 call uses
 // FP32 only after emission (not ImageBackward) and outside the fluid grid.
 // Before that, the adaptive step sequence decides where the backward ray
@@ -30,7 +30,8 @@
 //   * fluid sampling, radiative transfer, scattering and the camera test
 //     (shared FP64 device code), so cell indices and Stokes updates follow
 //     the FP64 form.
-#include "grt_launch.h"
+#pragma once
+
 #include "grt_metric_fast.cuh"
 #include "grt_trace.cuh"
 
@@ -74,49 +75,4 @@ struct MixedRhs {
 };
 
 }  // namespace dev
-
-// 128-thread blocks; MINB resident blocks per SM caps the registers per
-// thread at 65536 / (128 * MINB): 255, 170 and 128 for MINB = 2, 3, 4.
-template <int INTEGRATOR, int MINB, bool SHARE>
-__global__ void __launch_bounds__(128, MINB) trace_mixed(const __grid_constant__ KParams kp) {
-    extern __shared__ double smem[];
-    dev::Axes ax;
-    dev::KStore kk;
-    dev::stage_grid(kp, smem, INTEGRATOR, ax, kk);
-    dev::trace_body<INTEGRATOR, dev::MixedRhs, false, SHARE>(kp, ax, kk);
-}
-
-template <int I, int B>
-static cudaError_t launch_trace_mixed_v(const KParams& kp, int blocks, size_t smem, cudaStream_t stream) {
-    if (kp.ngroups > 0) {
-        cudaFuncSetAttribute(trace_mixed<I, B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        trace_mixed<I, B, true><<<blocks, 128, smem, stream>>>(kp);
-    } else {
-        cudaFuncSetAttribute(trace_mixed<I, B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        trace_mixed<I, B, false><<<blocks, 128, smem, stream>>>(kp);
-    }
-    return cudaGetLastError();
-}
-
-// 128-thread blocks, sm_count * blocks_per_sm of them; blocks_per_sm (2, 3
-// or 4) selects the register-capped instantiation.
-cudaError_t launch_trace_mixed(const KParams& kp, int integrator, int sm_count, int blocks_per_sm, size_t smem,
-                           cudaStream_t stream) {
-    const int blocks = sm_count * blocks_per_sm;
-    if (integrator == 0) {
-        switch (blocks_per_sm) {
-            case 2: return launch_trace_mixed_v<0, 2>(kp, blocks, smem, stream);
-            case 3: return launch_trace_mixed_v<0, 3>(kp, blocks, smem, stream);
-            case 4: return launch_trace_mixed_v<0, 4>(kp, blocks, smem, stream);
-            default: return cudaErrorInvalidConfiguration;
-        }
-    }
-    switch (blocks_per_sm) {
-        case 2: return launch_trace_mixed_v<1, 2>(kp, blocks, smem, stream);
-        case 3: return launch_trace_mixed_v<1, 3>(kp, blocks, smem, stream);
-        case 4: return launch_trace_mixed_v<1, 4>(kp, blocks, smem, stream);
-        default: return cudaErrorInvalidConfiguration;
-    }
-}
-
 }  // namespace grt

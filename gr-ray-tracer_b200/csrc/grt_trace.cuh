@@ -66,6 +66,7 @@ struct Lane {
     double radius;        // ks_radius of s, valid when have_radius
     uint64_t id;
     long long idx;        // photon index, -1 when idle
+    long long q;          // queue index of the lane's photon (geodesic index when sharing)
     long long calls;      // calls taken in this launch
     int phase;
     int have_radius;
@@ -356,7 +357,9 @@ GRT_DEV bool generate_packet(const KParams& kp, const FluidSample& fs, uint64_t 
 // SHARE: the lane also carries the other channels of its group (their
 // frequencies and Stokes vectors in their photon slots); *ch_term counts the
 // channels that terminated on their own in this call.
-template <bool RAW = false, class Rec = NoRecord, bool SHARE = false>
+// LEG (see trace_body) removes the code the leg never runs: generation from
+// the forward leg, transfer and the camera from the backward leg.
+template <bool RAW = false, class Rec = NoRecord, bool SHARE = false, int LEG = 0>
 GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, double taken, int64_t step,
                       double& tdisp, double& pdisp, int& have_disp, Rec rec = Rec(), int* ch_term = nullptr) {
     const KImage& im = image_params(kp, L.img);
@@ -367,7 +370,7 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
     FluidSample fs;
     const bool sampled = needs && sample_fluid<RAW>(kp, ax, L.s, L.radius, fs);
     int terminated = 0;
-    if (kp.image_mode && backward && sampled) {
+    if (LEG != 2 && kp.image_mode && backward && sampled) {
         double nu = 0.0, E = 0.0;
         const double dcode = fs.fluid.density_g_cm3 / kp.density_scale;
         const int packets = ComputeSuperphotonsPerCell(dcode, kp.norm);
@@ -428,7 +431,7 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
             L.phase = 4;  // Rejected
             terminated = 1;
         }
-    } else if (sampled && !backward) {
+    } else if (LEG != 1 && sampled && !backward) {
         const double I_before = L.I[0];
         double tau0 = 0.0, j0 = 0.0, att = 1.0, scale = 1.0;
         if (kp.abs_on) {
@@ -486,7 +489,7 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
         }
         rec.rt_step(fs.cell, tau0, j0, I_before, att, scale);
     }
-    if (kp.image_mode && phase0 == 2) {  // ImageForward
+    if (LEG != 1 && kp.image_mode && phase0 == 2) {  // ImageForward
         double u = 0.0, v = 0.0;
         const int crossing = camera_crossing(im, L.s, u, v);
         if (crossing > 0) {
@@ -521,8 +524,29 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
     return terminated;
 }
 
+// State of a live photon that the next launch over the queue needs besides
+// its photon slot: the calls taken (backward leg to forward leg) and, when
+// channels share the geodesic, which channel leads and which finished.
+template <bool SHARE, int LEG>
+GRT_DEV void store_carry(const KParams& kp, const Lane& L) {
+    if (LEG == 1) kp.calls_carry[L.q] = L.calls;
+    if (SHARE && kp.share_state)
+        kp.share_state[L.q] = (static_cast<unsigned long long>(L.lead) << 32) | L.done;
+}
+
 // SHARE: queue indices are geodesics of channel groups (KParams::ngroups > 0).
-template <int INTEGRATOR, class RHS, bool RAW = false, bool SHARE = false>
+// LEG splits an image-mode launch into two launches over the same queue:
+//   0  whole rays (disk mode, or image mode in one launch);
+//   1  the backward leg: photons in ImageBackward only; a lane hands its
+//      photon over when a call leaves it in another phase (after generation)
+//      -- stored like a budget end, with the calls taken so far in
+//      KParams::calls_carry[q];
+//   2  everything after: photons in any live phase but ImageBackward, resuming
+//      with the calls the backward launch left in calls_carry[q].
+// Each photon takes the same calls in the same order either way, so the two
+// launches give the one-launch result bit for bit; each loop body holds only
+// its own leg's code.
+template <int INTEGRATOR, class RHS, bool RAW = false, bool SHARE = false, int LEG = 0>
 GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -579,16 +603,22 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                         }
                         L.grp = lo;
                         L.pix = q - static_cast<long long>(kp.group_qstart[lo]);
-                        L.lead = 0;
                         L.nchan = kp.group_chan[lo + 1] - kp.group_chan[lo];
-                        L.done = 0;
+                        // which channel leads and which finished on their own,
+                        // as an earlier launch left them (zero after an init)
+                        const unsigned long long ss = kp.share_state ? kp.share_state[q] : 0ull;
+                        L.done = static_cast<unsigned>(ss & 0xFFFFFFFFull);
+                        L.lead = static_cast<int>((ss >> 32) & 0xFFull);
                         L.zero_all = 0;
-                        slot = chan_slot(kp, lo, 0, L.pix);
+                        slot = chan_slot(kp, lo, L.lead, L.pix);
                     }
-                    if (q >= 0 && !kp.ph.terminate[slot]) {
+                    if (q >= 0 && !kp.ph.terminate[slot] &&
+                        (LEG == 0 || ((kp.ph.phase[slot] == 1) == (LEG == 1)))) {
                         load_photon(kp.ph, slot, L);
                         L.idx = slot;
-                        L.img = SHARE ? chan_image(kp, L.grp, 0) : image_of_photon(kp, q);
+                        L.q = q;
+                        if (LEG == 2) L.calls = kp.calls_carry[q];
+                        L.img = SHARE ? chan_image(kp, L.grp, L.lead) : image_of_photon(kp, q);
                         have_disp = 0;
                     }
                 }
@@ -629,20 +659,21 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                     RHS::after_accept(L.s, kp, 1);
                     ++cnt.accepted;
                     int ch_term = 0;
-                    terminated = post_step<RAW, NoRecord, SHARE>(kp, ax, L, phase0, taken, kp.step0 + L.calls - 1,
-                                                                 tdisp, pdisp, have_disp, NoRecord(), &ch_term);
+                    terminated = post_step<RAW, NoRecord, SHARE, LEG>(kp, ax, L, phase0, taken,
+                                                                      kp.step0 + L.calls - 1, tdisp, pdisp, have_disp,
+                                                                      NoRecord(), &ch_term);
                     if (SHARE && ch_term) {
                         cnt.terminated += ch_term;
                         const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
                         if (ts > cnt.max_term_step) cnt.max_term_step = ts;
                     }
-                    finished = terminated;
+                    finished = terminated || (LEG == 1 && L.phase != 1);
                 } else {
                     // Mixed form: an RK45 call may use the FP32 right-hand side only
                     // when its step sequence cannot change which fluid cell the ray
                     // samples next: after emission (not ImageBackward) and outside
                     // the fluid grid.  Fixed-step RK4 calls may use it everywhere.
-                    L.fast = (L.phase != 1 && r * r > kp.fp32_min_radius_sq) ? 1 : 0;
+                    L.fast = (LEG != 1 && L.phase != 1 && r * r > kp.fp32_min_radius_sq) ? 1 : 0;
                     L.need_k1 = 1;
                     L.dl_try = L.dl;
                     L.attempts = 0;
@@ -652,7 +683,9 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
         }
         if (INTEGRATOR == 1 && L.mid_call) {
             const double taken = L.dl_try;
-            const int ok = rk45_attempt<RHS>(kp, L.s, &L.dl_try, L.k1, L.need_k1, L.fast, kk);
+            // the backward leg never uses the FP32 right-hand side (a literal
+            // 0 lets the compiler drop it from the backward kernel)
+            const int ok = rk45_attempt<RHS>(kp, L.s, &L.dl_try, L.k1, L.need_k1, LEG == 1 ? 0 : L.fast, kk);
             L.need_k1 = 0;
             ++L.attempts;
             if (ok) {
@@ -662,14 +695,14 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                 L.mid_call = 0;
                 const int phase0 = L.phase;
                 int ch_term = 0;
-                terminated = post_step<RAW, NoRecord, SHARE>(kp, ax, L, phase0, taken, kp.step0 + L.calls - 1, tdisp,
-                                                             pdisp, have_disp, NoRecord(), &ch_term);
+                terminated = post_step<RAW, NoRecord, SHARE, LEG>(kp, ax, L, phase0, taken, kp.step0 + L.calls - 1,
+                                                                  tdisp, pdisp, have_disp, NoRecord(), &ch_term);
                 if (SHARE && ch_term) {
                     cnt.terminated += ch_term;
                     const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
                     if (ts > cnt.max_term_step) cnt.max_term_step = ts;
                 }
-                finished = terminated;
+                finished = terminated || (LEG == 1 && L.phase != 1);
             } else {
                 ++cnt.rejected;
                 if (L.attempts >= 12) {
@@ -685,13 +718,18 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                 cnt.terminated += stored;
                 const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
                 if (ts > cnt.max_term_step) cnt.max_term_step = ts;
+            } else {
+                store_carry<SHARE, LEG>(kp, L);
             }
             L.idx = -1;
         }
     }
     if (timed_out) {
         // Leave every photon consistent: write back what this lane holds.
-        if (L.idx >= 0) store_all<SHARE>(kp, L, 0, tdisp, pdisp, have_disp);
+        if (L.idx >= 0) {
+            store_all<SHARE>(kp, L, 0, tdisp, pdisp, have_disp);
+            store_carry<SHARE, LEG>(kp, L);
+        }
         if (lane == 0) atomicAdd(&kp.counters->timed_out, 1ull);
     }
     // ---- flush counters: warp reduce, one atomic per counter per warp ----

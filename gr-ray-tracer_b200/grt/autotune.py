@@ -2,8 +2,9 @@
 
 Searches the occupancy class (resident 128-thread blocks per SM, i.e. the
 register cap of the kernel instantiation), the per-warp refill threshold (idle
-lanes before a warp pulls new photons) and the photons a warp claims per queue
-access, timing each candidate with the library's own CUDA
+lanes before a warp pulls new photons), the photons a warp claims per queue
+access and, in image mode, whether the rays' backward and forward legs run as
+two launches or one, timing each candidate with the library's own CUDA
 events around the trace launch on the actual workload.  Results are cached per
 (workload key, precision, integrator) for the life of the process.
 """
@@ -17,13 +18,17 @@ _CACHE: dict = {}
 BLOCKS_PER_SM = (2, 3, 4)   # 128-thread blocks; register caps 255 / 170 / 128
 REFILL = (1, 8, 16, 32)
 GRAB = (32, 128)
+SPLIT_LEGS = (1, 0)         # image mode: backward leg and the rest as two launches, or one
 
 
-def candidates():
+def candidates(image_mode: bool = True):
     """Occupancy classes (resident 128-thread blocks per SM, which fix the
-    register cap of the instantiation) crossed with the queue knobs."""
-    for bps, refill, grab in itertools.product(BLOCKS_PER_SM, REFILL, GRAB):
-        yield dict(threads_per_block=128, blocks_per_sm=bps, refill_threshold=refill, photons_per_grab=grab)
+    register cap of the instantiation) crossed with the queue knobs and, in
+    image mode, the leg split."""
+    for bps, refill, grab, split in itertools.product(BLOCKS_PER_SM, REFILL, GRAB,
+                                                      SPLIT_LEGS if image_mode else (0,)):
+        yield dict(threads_per_block=128, blocks_per_sm=bps, refill_threshold=refill, photons_per_grab=grab,
+                   split_legs=split)
 
 
 def tune(ctx, prepare, key, reps: int = 2, log=None):
@@ -40,7 +45,8 @@ def tune(ctx, prepare, key, reps: int = 2, log=None):
         return cfg, ms, table
     table = []
     best = None
-    for cfg in candidates():
+    from .abi import MODE_IMAGE
+    for cfg in candidates(ctx.params.mode == MODE_IMAGE):
         ctx.set_launch_config(**cfg)
         prepare(ctx)
         ctx.run()

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define GRT_ABI_VERSION 2
+#define GRT_ABI_VERSION 3
 
 typedef enum grt_status {
     GRT_OK = 0,
@@ -160,6 +160,9 @@ typedef struct grt_launch_config {
     int32_t blocks_per_sm;        /* 2, 3 or 4 resident blocks per SM: register caps 255 / 170 / 128 */
     int32_t refill_threshold;     /* idle lanes in a warp before it pulls new photons (1..32) */
     int32_t photons_per_grab;     /* photons a warp claims per access to the global queue */
+    int32_t split_legs;           /* image mode: 1 = trace the backward leg of every ray in one launch and
+                                     the rest in a second (same results, smaller loop bodies); 0 = one
+                                     launch for whole rays */
 } grt_launch_config;
 
 typedef struct grt_ctx grt_ctx;

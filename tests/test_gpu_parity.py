@@ -37,7 +37,7 @@ def test_image_parity_fp64(gpu, oracle, w):
 
 
 @pytest.mark.parametrize("launch", [
-    dict(threads_per_block=128, blocks_per_sm=2, refill_threshold=1, photons_per_grab=32),
+    dict(threads_per_block=128, blocks_per_sm=2, refill_threshold=1, photons_per_grab=32, split_legs=0),
     dict(threads_per_block=128, blocks_per_sm=3, refill_threshold=16, photons_per_grab=64),
     dict(threads_per_block=128, blocks_per_sm=4, refill_threshold=32, photons_per_grab=4096),
 ])
