@@ -143,6 +143,10 @@ struct grt_ctx {
     DevBuf<int> group_chan_dev, chan_img_dev;
     DevBuf<unsigned long long> share_state;  // [geodesics] lead / finished channels (KParams::share_state)
     DevBuf<long long> calls_carry;           // [queue] calls taken in the backward-leg launch
+    // output-step archives: gathered fields on the device, then in pinned host memory
+    DevBuf<unsigned char> out_stage;
+    unsigned char* host_out = nullptr;
+    size_t host_out_bytes = 0;
     // per-image products of a batch: image k's I,Q,U,V at bimage + bimage_off[k]
     DevBuf<double> bimage, bspectrum;
     DevBuf<unsigned long long> barrived;
@@ -384,6 +388,8 @@ void grt_destroy(grt_ctx* c) {
     c->ckpt.release(); c->tape.release(); c->dLdI.release(); c->g_abs.release(); c->g_emis.release();
     c->nckpt.release(); c->adj_overflow.release(); c->call0.release();
     c->bimage.release(); c->bspectrum.release(); c->barrived.release();
+    c->share_state.release(); c->calls_carry.release(); c->out_stage.release();
+    if (c->host_out) cudaFreeHost(c->host_out);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->host_counters) cudaFreeHost(c->host_counters);
@@ -1071,8 +1077,25 @@ grt_status grt_get_batch_image_products(grt_ctx* c, size_t image, grt_image_prod
     return GRT_OK;
 }
 
-grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
-    if (!c) return GRT_EINVAL;
+}  // extern "C"
+
+namespace {
+
+// Where run_steps writes output-step archives (nullptr: none).
+struct OutputPlan {
+    std::string dir, name;
+    std::vector<int> fields;
+    uint64_t stride;
+    int32_t rank;
+};
+
+grt_status write_output_step(grt_ctx* c, const OutputPlan& plan, int64_t step);
+
+// The step loop of integrate_geodesics (integrate_cart_ks.hpp:468-527).
+// Without output and with termination_percent = 1 one launch covers it; else
+// launches end on the output steps, where the terminated fraction is checked
+// (and, with a plan, an archive written).
+grt_status run_steps(grt_ctx* c, grt_run_stats* stats, const OutputPlan* plan) {
     if (!c->grid_uploaded) return fail(c, GRT_ESTATE, "grt_run before grt_upload_grid");
     const grt_params& p = c->p;
     grt_run_stats st;
@@ -1101,7 +1124,7 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
     // (integrate_cart_ks.hpp:491-526).  With termination_percent = 1 the check
     // can only succeed once every photon has terminated, so one launch covers
     // the whole loop.
-    const bool single = p.termination_percent >= 1.0;
+    const bool single = p.termination_percent >= 1.0 && !plan;
     int64_t step = 0;
     int64_t steps_done = 0;
     unsigned long long max_term_step = 0;
@@ -1146,6 +1169,10 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
         }
         step = end;
         steps_done = end;
+        if (plan) {
+            const grt_status ws = write_output_step(c, *plan, end - 1);
+            if (ws != GRT_OK) return ws;
+        }
         const double fraction = static_cast<double>(terminated) / static_cast<double>(total);
         if (fraction >= p.termination_percent) break;
     }
@@ -1155,6 +1182,15 @@ grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
     st.trace_ms = ms_total;
     if (stats) *stats = st;
     return GRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
+    if (!c) return GRT_EINVAL;
+    return run_steps(c, stats, nullptr);
 }
 
 grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
@@ -1444,6 +1480,97 @@ grt_status write_products_archive(grt_ctx* c, const std::string& output_dir, con
     return GRT_OK;
 }
 
+// Device pointer and element size of output field k (grt::kOutputFields order).
+const void* output_field(const grt_ctx* c, int k, int& item) {
+    item = 8;
+    if (k == 0) return c->ph.id.ptr;
+    if (k >= 1 && k <= 15) return c->ph.f[k - 1].ptr;  // frequency .. dlambda
+    if (k == 16 || k == 17) {
+        item = 1;
+        return k == 16 ? static_cast<const void*>(c->ph.term.ptr) : static_cast<const void*>(c->ph.phase.ptr);
+    }
+    return c->ph.f[k - 3].ptr;  // 18, 19: theta_disp, phi_disp
+}
+
+// write_output_step (write_output.hpp:90-103) with add_photon_array's strided
+// values (:26-59): the selected fields of photons 0, stride, 2*stride, ...
+// gathered on the device into one staging buffer, one copy back, then one
+// archive written under a temporary name and renamed into place.
+grt_status write_output_step(grt_ctx* c, const OutputPlan& plan, int64_t step) {
+    namespace fs = std::filesystem;
+    const size_t n = c->n;
+    const unsigned long long count = n == 0 ? 0 : 1 + (n - 1) / plan.stride;
+    grt::GatherArgs g;
+    std::memset(&g, 0, sizeof(g));
+    unsigned long long bytes = 0;
+    for (size_t q = 0; q < plan.fields.size(); ++q) {
+        g.src[q] = output_field(c, plan.fields[q], g.item[q]);
+        g.dst_off[q] = bytes;
+        bytes += (count * g.item[q] + 7) / 8 * 8;
+    }
+    g.nfields = static_cast<int>(plan.fields.size());
+    g.count = count;
+    g.stride = plan.stride;
+    if (bytes > 0) {
+        GRT_CUDA(c, c->out_stage.alloc(bytes), "alloc output stage");
+        if (c->host_out_bytes < bytes) {
+            if (c->host_out) cudaFreeHost(c->host_out);
+            c->host_out = nullptr;
+            c->host_out_bytes = 0;
+            GRT_CUDA(c, cudaMallocHost(reinterpret_cast<void**>(&c->host_out), bytes), "alloc output host stage");
+            c->host_out_bytes = bytes;
+        }
+        g.dst = c->out_stage.ptr;
+        GRT_CUDA(c, grt::launch_gather_fields(g, c->sm_count, c->stream), "gather_fields");
+        GRT_CUDA(c, cudaMemcpyAsync(c->host_out, c->out_stage.ptr, bytes, cudaMemcpyDeviceToHost, c->stream),
+                 "D2H output step");
+        GRT_CUDA(c, cudaStreamSynchronize(c->stream), "output step");
+    }
+    std::error_code ec;
+    fs::create_directories(plan.dir, ec);
+    const fs::path final_path =
+        fs::path(plan.dir) / (plan.name + "_step_" + std::to_string(step) + "_rank" + std::to_string(plan.rank) + ".npz");
+    const fs::path tmp = final_path.string() + ".tmp";
+    grt::NpzOut z;
+    if (!z.open(tmp.string())) return fail(c, GRT_EIO, "Failed to open output NumPy archive: " + tmp.string());
+    const std::vector<size_t> shape{static_cast<size_t>(count)};
+    bool ok = true;
+    for (size_t q = 0; q < plan.fields.size() && ok; ++q) {
+        const int k = plan.fields[q];
+        const char* descr = k == 0 ? "<u8" : (g.item[q] == 1 ? "|u1" : "<f8");
+        ok = z.add(grt::kOutputFields[k], grt::npy_bytes(descr, shape, c->host_out ? c->host_out + g.dst_off[q] : nullptr,
+                                                         static_cast<size_t>(g.item[q])));
+    }
+    ok = z.close() && ok;
+    if (!ok) {
+        fs::remove(tmp, ec);
+        return fail(c, GRT_EIO, "Failed while writing NumPy archive");
+    }
+    fs::rename(tmp, final_path, ec);
+    if (ec) {
+        fs::remove(tmp, ec);
+        return fail(c, GRT_EIO, "Failed to publish output archive " + final_path.string() + ": " + ec.message());
+    }
+    return GRT_OK;
+}
+
+grt_status make_output_plan(grt_ctx* c, const char* output_dir, const char* name, const char* variables,
+                            uint64_t stride, int32_t rank, OutputPlan& plan) {
+    if (!output_dir || !name || !variables) return fail(c, GRT_EINVAL, "null output argument");
+    if (!*output_dir) return fail(c, GRT_EINVAL, "output.directory must not be empty");
+    if (!*name) return fail(c, GRT_EINVAL, "simulation.name must not be empty");
+    if (stride == 0) return fail(c, GRT_EINVAL, "output.stride must be positive");
+    std::string err;
+    if (!grt::parse_output_variables(variables, plan.fields, err)) return fail(c, GRT_EINVAL, err);
+    if (plan.fields.size() > static_cast<size_t>(grt::kGatherMaxFields))
+        return fail(c, GRT_EINVAL, "too many output variables");
+    plan.dir = output_dir;
+    plan.name = name;
+    plan.stride = stride;
+    plan.rank = rank;
+    return GRT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1476,6 +1603,30 @@ grt_status grt_write_batch_products_npz(grt_ctx* c, const char* output_dir, cons
                                    bins, out);
         if (s != GRT_OK) return s;
     }
+    return GRT_OK;
+}
+
+grt_status grt_write_output_step_npz(grt_ctx* c, const char* output_dir, const char* name, int64_t step,
+                                     int32_t rank, const char* variables, uint64_t stride) {
+    if (!c) return GRT_EINVAL;
+    OutputPlan plan;
+    const grt_status ps = make_output_plan(c, output_dir, name, variables, stride, rank, plan);
+    if (ps != GRT_OK) return ps;
+    return write_output_step(c, plan, step);
+}
+
+grt_status grt_run_with_output(grt_ctx* c, const char* output_dir, const char* name, const char* variables,
+                               uint64_t stride, grt_run_stats* stats) {
+    if (!c) return GRT_EINVAL;
+    OutputPlan plan;
+    grt_status s = make_output_plan(c, output_dir, name, variables, stride, c->p.rank, plan);
+    if (s != GRT_OK) return s;
+    s = run_steps(c, stats, &plan);
+    if (s != GRT_OK) return s;
+    // integrate_cart_ks.hpp:529-531: image mode ends with the image products
+    if (c->p.mode == GRT_MODE_IMAGE)
+        return c->batched ? grt_write_batch_products_npz(c, output_dir, name)
+                          : grt_write_image_products_npz(c, output_dir, name);
     return GRT_OK;
 }
 

@@ -13,6 +13,8 @@
 //     so archives are byte-for-byte the ones the reference writes.
 #include "grt_host.h"
 
+#include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -308,6 +310,52 @@ grt_status grt_params_from_toml(const char* path, grt_params* p, char* numpy_dir
     return GRT_OK;
 }
 
+grt_status grt_output_options_from_toml(const char* path, char* variables, size_t variables_len, uint64_t* stride,
+                                        char* err, size_t err_len) {
+    if (!path) {
+        set_err(err, err_len, "null argument");
+        return GRT_EINVAL;
+    }
+    try {
+        const Raw c = parse_flat(path);
+        const std::string spec = get_str(c, "output.variables", "id,frequency,x0,x1,x2,x3,k0,k1,k2,k3,I,Q,U,V,phase");
+        const uint64_t st = get_u64(c, "output.stride", 1);
+        if (st == 0) throw std::runtime_error("output.stride must be positive");
+        std::vector<int> fields;
+        std::string msg;
+        if (!grt::parse_output_variables(spec, fields, msg)) throw std::runtime_error(msg);
+        if (variables && variables_len) {
+            if (spec.size() + 1 > variables_len) throw std::runtime_error("output.variables longer than the buffer");
+            set_str(variables, variables_len, spec);
+        }
+        if (stride) *stride = st;
+    } catch (const std::runtime_error& e) {
+        set_err(err, err_len, e.what());
+        return std::string(e.what()).rfind("Failed to open config file", 0) == 0 ? GRT_EIO : GRT_EINVAL;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, std::string("invalid config value: ") + e.what());
+        return GRT_EINVAL;
+    }
+    return GRT_OK;
+}
+
+grt_status grt_parse_output_variables(const char* spec, int32_t* fields, size_t* count, char* err, size_t err_len) {
+    if (!spec || !count) {
+        set_err(err, err_len, "null argument");
+        return GRT_EINVAL;
+    }
+    std::vector<int> f;
+    std::string msg;
+    if (!grt::parse_output_variables(spec, f, msg)) {
+        set_err(err, err_len, msg);
+        return GRT_EINVAL;
+    }
+    if (fields)
+        for (size_t k = 0; k < f.size(); ++k) fields[k] = f[k];
+    *count = f.size();
+    return GRT_OK;
+}
+
 }  // extern "C"
 
 namespace grt {
@@ -426,6 +474,60 @@ std::vector<char> npy_bytes(const char* descr, const std::vector<size_t>& shape,
     const char* raw = static_cast<const char*>(data);
     b.insert(b.end(), raw, raw + total * item_size);
     return b;
+}
+
+const char* const kOutputFields[kOutputFieldCount] = {
+    "id", "frequency", "emission_frame_energy", "x0", "x1", "x2", "x3", "k0", "k1", "k2", "k3",
+    "I", "Q", "U", "V", "dlambda", "terminate", "phase", "theta_disp", "phi_disp"};
+
+namespace {
+std::string trim_spaces(const std::string& v) {
+    size_t a = 0, b = v.size();
+    while (a < b && std::isspace(static_cast<unsigned char>(v[a]))) ++a;
+    while (b > a && std::isspace(static_cast<unsigned char>(v[b - 1]))) --b;
+    return v.substr(a, b - a);
+}
+}  // namespace
+
+bool parse_output_variables(const std::string& spec_in, std::vector<int>& fields, std::string& err) {
+    fields.clear();
+    std::string spec = trim_spaces(spec_in);
+    if (spec.empty()) {
+        err = "output variables cannot be empty";
+        return false;
+    }
+    if (spec.size() >= 2 && spec.front() == '[' && spec.back() == ']') spec = spec.substr(1, spec.size() - 2);
+    size_t begin = 0;
+    while (begin <= spec.size()) {
+        const size_t comma = spec.find(',', begin);
+        std::string name = trim_spaces(spec.substr(begin, comma == std::string::npos ? std::string::npos : comma - begin));
+        if (name.size() >= 2 && ((name.front() == '"' && name.back() == '"') ||
+                                 (name.front() == '\'' && name.back() == '\'')))
+            name = trim_spaces(name.substr(1, name.size() - 2));
+        if (name == "all") {
+            // appended to what came before, as the reference does (so "I,all"
+            // writes I twice)
+            for (int k = 0; k < kOutputFieldCount; ++k) fields.push_back(k);
+            return true;
+        }
+        if (!name.empty()) {
+            int k = 0;
+            while (k < kOutputFieldCount && name != kOutputFields[k]) ++k;
+            if (k == kOutputFieldCount) {
+                err = "unknown output variable: " + name;
+                fields.clear();
+                return false;
+            }
+            if (std::find(fields.begin(), fields.end(), k) == fields.end()) fields.push_back(k);
+        }
+        if (comma == std::string::npos) break;
+        begin = comma + 1;
+    }
+    if (fields.empty()) {
+        err = "output variables cannot be empty";
+        return false;
+    }
+    return true;
 }
 
 bool NpzOut::open(const std::string& path) {

@@ -16,6 +16,18 @@ bool npy_load_f64(const std::string& path, std::vector<size_t>& shape, std::vect
 std::vector<char> npy_bytes(const char* descr, const std::vector<size_t>& shape, const void* data,
                             size_t item_size);
 
+// The photon fields an output step can write, in the reference's order
+// (available_output_variables, src/output/output_variables.hpp:12-18).
+constexpr int kOutputFieldCount = 20;
+extern const char* const kOutputFields[kOutputFieldCount];
+
+// OutputSelection::parse (output_variables.hpp:27-70): field indices into
+// kOutputFields in the order written (at most kMaxOutputSelection: up to 20
+// distinct names, then "all" appends all 20); false with the reference's
+// message on an unknown or empty selection.
+constexpr int kMaxOutputSelection = 2 * kOutputFieldCount;
+bool parse_output_variables(const std::string& spec, std::vector<int>& fields, std::string& err);
+
 // Uncompressed (STORED) .npz writer.
 class NpzOut {
 public:

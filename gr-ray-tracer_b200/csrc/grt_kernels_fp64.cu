@@ -5,6 +5,7 @@
 //   image_products        -- build_observation_products (observation.hpp:31-84)
 //   init_disk_photons     -- initialize_photons_disk (initialize_photons.hpp:173-327)
 //   count_terminated      -- "Count Terminated Photons" (integrate_cart_ks.hpp:496-503)
+//   gather_fields         -- strided field gather of write_output_step (write_output.hpp:13-59)
 //
 // and the dispatcher over the trace kernels of grt_trace_inst.cu.
 #include "grt_launch.h"
@@ -197,7 +198,33 @@ __global__ void init_disk_photons(const __grid_constant__ DiskInitArgs args) {
     P.phi_disp[i] = 0.0;
 }
 
+// make_strided_host_values (write_output.hpp:13-24) for every selected field
+// at once: blockIdx.y picks the field; 8-byte fields copy as 64-bit words.
+__global__ void gather_fields(const __grid_constant__ GatherArgs a) {
+    const int f = blockIdx.y;
+    const unsigned long long step = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+    for (unsigned long long j = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; j < a.count;
+         j += step) {
+        const unsigned long long i = j * a.stride;
+        if (a.item[f] == 8)
+            reinterpret_cast<unsigned long long*>(a.dst + a.dst_off[f])[j] =
+                static_cast<const unsigned long long*>(a.src[f])[i];
+        else
+            a.dst[a.dst_off[f] + j] = static_cast<const unsigned char*>(a.src[f])[i];
+    }
+}
+
 // ---- host-side launchers ----
+cudaError_t launch_gather_fields(const GatherArgs& a, int sm_count, cudaStream_t stream) {
+    if (a.count == 0 || a.nfields == 0) return cudaSuccess;
+    if (a.nfields > kGatherMaxFields) return cudaErrorInvalidValue;
+    const unsigned long long want = (a.count + 255) / 256;
+    const unsigned long long cap = static_cast<unsigned long long>(sm_count) * 8;
+    const dim3 grid(static_cast<unsigned>(want < cap ? want : cap), static_cast<unsigned>(a.nfields));
+    gather_fields<<<grid, 256, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_trace(const KParams& kp, bool mixed, int leg, int integrator, int sm_count, int blocks_per_sm,
                          size_t smem, cudaStream_t stream) {
     const int blocks = sm_count * blocks_per_sm;

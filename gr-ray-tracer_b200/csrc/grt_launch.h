@@ -75,6 +75,19 @@ struct ProductsSet {
     ProductsImage img[kProductsMaxImages];
 };
 
+// Strided gather of an output step's photon fields (write_output_step):
+// elements src[k][j * stride], j < count, of field k packed at dst + dst_off[k].
+constexpr int kGatherMaxFields = 40;  // a selection's fields, "all" after 20 names included
+struct GatherArgs {
+    const void* src[kGatherMaxFields];
+    unsigned long long dst_off[kGatherMaxFields];
+    int item[kGatherMaxFields];  // element bytes: 8 or 1
+    int nfields;
+    int pad;
+    unsigned long long count, stride;
+    unsigned char* dst;
+};
+
 // Buffers of the adjoint pass (grt_adjoint.cu).
 struct AdjointArgs {
     double* ckpt;              // [n][cap][16] ray state after emission and every K calls
@@ -151,6 +164,7 @@ cudaError_t launch_init_image(const InitImageArgs& args, cudaStream_t stream);
 cudaError_t launch_init_disk(const DiskInitArgs& a, cudaStream_t stream);
 // Fills block0 / blocks of `set` and launches it.
 cudaError_t launch_image_products(ProductsSet& set, cudaStream_t stream);
+cudaError_t launch_gather_fields(const GatherArgs& a, int sm_count, cudaStream_t stream);
 cudaError_t launch_count_terminated(const uint8_t* term, unsigned long long n, unsigned long long* out,
                                     int sm_count, cudaStream_t stream);
 

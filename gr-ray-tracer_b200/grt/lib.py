@@ -94,7 +94,13 @@ def load(path: Path | None = None):
     L.grt_set_cell_multipliers.argtypes = [vp, P(C.c_double), P(C.c_double)]
     L.grt_forward_checkpointed.argtypes = [vp, C.c_int64, P(RunStats)]
     L.grt_adjoint_image_I.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_double)]
-    for name in ("grt_set_cell_multipliers", "grt_forward_checkpointed", "grt_adjoint_image_I",
+    L.grt_parse_output_variables.argtypes = [C.c_char_p, P(C.c_int32), P(C.c_size_t), C.c_char_p, C.c_size_t]
+    L.grt_output_options_from_toml.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t, P(C.c_uint64), C.c_char_p,
+                                               C.c_size_t]
+    L.grt_write_output_step_npz.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int64, C.c_int32, C.c_char_p, C.c_uint64]
+    L.grt_run_with_output.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64, P(RunStats)]
+    for name in ("grt_parse_output_variables", "grt_output_options_from_toml", "grt_write_output_step_npz",
+                 "grt_run_with_output", "grt_set_cell_multipliers", "grt_forward_checkpointed", "grt_adjoint_image_I",
                  "grt_init_image_batch", "grt_get_batch_image_products", "grt_write_batch_products_npz",
                  "grt_render_graph", "grt_trace_device_noalloc", "grt_measure_fma_peaks", "grt_params_validate", "grt_params_from_toml", "grt_create", "grt_set_params",
                  "grt_set_stream", "grt_synchronize", "grt_upload_grid", "grt_upload_grid_numpy_dir",
@@ -110,6 +116,34 @@ def default_params() -> Params:
     p = Params()
     load().grt_params_default(C.byref(p))
     return p
+
+
+# The photon fields an output step can write, in the reference's order.
+OUTPUT_FIELDS = ("id", "frequency", "emission_frame_energy", "x0", "x1", "x2", "x3", "k0", "k1", "k2", "k3",
+                 "I", "Q", "U", "V", "dlambda", "terminate", "phase", "theta_disp", "phi_disp")
+DEFAULT_OUTPUT_VARIABLES = "id,frequency,x0,x1,x2,x3,k0,k1,k2,k3,I,Q,U,V,phase"
+
+
+def parse_output_variables(spec: str) -> list:
+    """OutputSelection::parse: the field names an output step writes, in order."""
+    fields = (C.c_int32 * (2 * len(OUTPUT_FIELDS)))()
+    count = C.c_size_t(0)
+    err = C.create_string_buffer(512)
+    rc = load().grt_parse_output_variables(spec.encode(), fields, C.byref(count), err, 512)
+    if rc != GRT_OK:
+        raise GrtError(rc, err.value.decode())
+    return [OUTPUT_FIELDS[fields[k]] for k in range(count.value)]
+
+
+def output_options_from_toml(path) -> tuple:
+    """(output.variables, output.stride) of a reference TOML config."""
+    buf = C.create_string_buffer(4096)
+    stride = C.c_uint64(0)
+    err = C.create_string_buffer(512)
+    rc = load().grt_output_options_from_toml(str(path).encode(), buf, 4096, C.byref(stride), err, 512)
+    if rc != GRT_OK:
+        raise GrtError(rc, err.value.decode())
+    return buf.value.decode(), int(stride.value)
 
 
 def validate_params(p: Params):
@@ -318,6 +352,20 @@ class Context:
 
     def write_image_products_npz(self, output_dir, name):
         self._check(self.lib.grt_write_image_products_npz(self._h, str(output_dir).encode(), name.encode()))
+
+    def write_output_step_npz(self, output_dir, name, step: int, rank: int = 0,
+                              variables: str = DEFAULT_OUTPUT_VARIABLES, stride: int = 1):
+        """<output_dir>/<name>_step_<step>_rank<rank>.npz of the current photons."""
+        self._check(self.lib.grt_write_output_step_npz(self._h, str(output_dir).encode(), name.encode(), int(step),
+                                                       int(rank), variables.encode(), int(stride)))
+
+    def run_with_output(self, output_dir, name, variables: str = DEFAULT_OUTPUT_VARIABLES, stride: int = 1) -> dict:
+        """The reference's step loop with an archive after every output step
+        (and the image products at the end in image mode)."""
+        st = RunStats()
+        self._check(self.lib.grt_run_with_output(self._h, str(output_dir).encode(), name.encode(), variables.encode(),
+                                                 int(stride), C.byref(st)))
+        return st.as_dict()
 
     def launch_config(self) -> dict:
         lc = LaunchConfig()

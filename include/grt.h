@@ -281,6 +281,54 @@ grt_status grt_get_image_products(grt_ctx* ctx, grt_image_products* out);
 grt_status grt_write_image_products_npz(grt_ctx* ctx, const char* output_dir, const char* name);
 
 /*
+ * Output-step archives (the reference's checkpoints).  The photon fields an
+ * output step can write, in the reference's order (available_output_variables,
+ * src/output/output_variables.hpp:12-18):
+ *   0 id, 1 frequency, 2 emission_frame_energy, 3-6 x0..x3, 7-10 k0..k3,
+ *   11-14 I Q U V, 15 dlambda, 16 terminate, 17 phase, 18 theta_disp, 19 phi_disp.
+ *
+ * grt_parse_output_variables is OutputSelection::parse (output_variables.hpp:
+ * 27-70): a comma list, optionally in [ ] with quoted names, duplicates
+ * dropped; "all" appends every field to the names before it and ends the list
+ * (as in the reference, a name before "all" is then written twice).  fields
+ * (may be NULL; room for 40) receives the indices in the order written,
+ * *count their number.  GRT_EINVAL with the
+ * reference's message ("unknown output variable: X", "output variables cannot
+ * be empty") otherwise.
+ *
+ * grt_output_options_from_toml reads output.variables (default
+ * "id,frequency,x0,x1,x2,x3,k0,k1,k2,k3,I,Q,U,V,phase") and output.stride
+ * (default 1, must be positive) of a reference TOML config
+ * (toml_config.hpp:225-243), validating the selection.
+ */
+grt_status grt_parse_output_variables(const char* spec, int32_t* fields, size_t* count, char* err, size_t err_len);
+grt_status grt_output_options_from_toml(const char* path, char* variables, size_t variables_len, uint64_t* stride,
+                                        char* err, size_t err_len);
+
+/*
+ * write_output_step (write_output.hpp:90-103): <output_dir>/<name>_step_<step>_rank<rank>.npz
+ * holding the selected fields of photons 0, stride, 2*stride, ... (each a 1-D
+ * array: id <u8, terminate and phase |u1, the rest <f8), written under a
+ * temporary name and renamed into place.  The fields are gathered on the
+ * device and copied back in one transfer.
+ */
+grt_status grt_write_output_step_npz(grt_ctx* ctx, const char* output_dir, const char* name, int64_t step,
+                                     int32_t rank, const char* variables, uint64_t stride);
+
+/*
+ * The reference's whole step loop with its output (integrate_geodesics,
+ * integrate_cart_ks.hpp:468-532): trace launches end on every output step
+ * (step % output_interval == 0, and the last step); after each, the
+ * terminated fraction is evaluated and the output-step archive written (rank
+ * p.rank); the loop stops once the fraction reaches termination_percent.  In
+ * image mode the image-products archive follows (grt_write_image_products_npz,
+ * or grt_write_batch_products_npz for a batch).  Per-photon results equal
+ * grt_run's.
+ */
+grt_status grt_run_with_output(grt_ctx* ctx, const char* output_dir, const char* name, const char* variables,
+                               uint64_t stride, grt_run_stats* stats);
+
+/*
  * Disk-mode emission, as initialize_photons_disk (initialize_photons.hpp:
  * 173-327) after build_superphoton_cell_offsets (:32-64): every grid cell
  * emits ComputeSuperphotonsPerCell(rho, superphoton_count_normalization)

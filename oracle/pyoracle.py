@@ -192,6 +192,7 @@ class Reference:
         L.ref_inverse_metric_deriv.argtypes = [_DP, C.c_double, C.c_double, _DP]
         L.ref_geodesic_observables.argtypes = [_DP, C.c_double, C.c_double, _DP]
         L.ref_locate_cell.argtypes = [C.c_size_t] * 3 + [_DP] * 3 + [C.c_double] * 3 + [C.POINTER(C.c_int)]
+        L.ref_parse_output_variables.argtypes = [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_size_t)]
 
     @staticmethod
     def available():
@@ -199,6 +200,14 @@ class Reference:
 
     def error(self):
         return self.lib.ref_last_error().decode()
+
+    def parse_output_variables(self, spec: str):
+        """The reference's OutputSelection::parse: field indices in write order."""
+        fields = (C.c_int32 * 40)()
+        count = C.c_size_t(0)
+        if self.lib.ref_parse_output_variables(spec.encode(), fields, C.byref(count)) != 0:
+            raise ValueError(self.error())
+        return [fields[k] for k in range(count.value)]
 
     def params_from_toml(self, path) -> Params:
         p = Params()

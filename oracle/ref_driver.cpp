@@ -21,6 +21,7 @@
 #include "radiative_transfer/initialize_photons.hpp"
 #include "geodesic_integrate/integrate_cart_ks.hpp"
 #include "analysis/geodesic_observables.hpp"
+#include "output/write_output.hpp"
 
 #include <chrono>
 #include <cstring>
@@ -343,6 +344,28 @@ int ref_locate_cell(std::size_t nr, std::size_t nth, std::size_t nph, const doub
     const bool ok = locate_structured_grid_cell(R, TH, PH, radius, polar, azimuth, i, j, k);
     ijk[0] = i; ijk[1] = j; ijk[2] = k;
     return ok ? 1 : 0;
+}
+
+// OutputSelection::parse of the reference (src/output/output_variables.hpp:
+// 27-70): the selected fields as indices into available_output_variables, in
+// the order the reference writes them (fields has room for 40).  Returns 0, or
+// 1 with the message.
+int ref_parse_output_variables(const char* spec, int32_t* fields, size_t* count) {
+    try {
+        const OutputSelection sel = OutputSelection::parse(spec);
+        size_t k = 0;
+        if (sel.names().size() > 40) throw std::runtime_error("more than 40 selected fields");
+        for (const std::string& name : sel.names()) {
+            int idx = 0;
+            while (available_output_variables[idx] != name) ++idx;
+            fields[k++] = idx;
+        }
+        *count = k;
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
 }
 
 }  // extern "C"
