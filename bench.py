@@ -538,13 +538,109 @@ def run_reference(args):
     }), flush=True)
 
 
+def timed_call(stream, fn):
+    """(result, ms) of fn() bracketed by CUDA events on `stream`."""
+    import torch
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    out = fn()
+    ev1.record(stream)
+    ev1.synchronize()
+    return out, ev0.elapsed_time(ev1)
+
+
+def run_adjoint(args):
+    """C4: the adjoint of the radiative-transfer sweep -- checkpointed forward
+    trace of the 128x128 line-of-sight image over the 96x48x48 torus, then the
+    reverse sweep for an L2 loss to a target rendered from perturbed
+    multipliers.  One step = forward + adjoint; reports rays/s of the pair."""
+    import numpy as np
+    import torch
+    from grt import lib, workloads
+    dist_setup(args.gpus)
+    w = workloads.C4
+    p = w.params()
+    grid = w.torus()
+    shape = grid["r.npy"].shape
+    stream = torch.cuda.Stream()
+    ta, te = workloads.c4_target_multipliers(shape)
+    ctx = lib.Context(p)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload_grid(grid)
+    ctx.set_cell_multipliers(ta, te)
+    ctx.init_image_forward_photons(p.image_nx, p.image_ny, workloads.C4_BACK_DISTANCE)
+    ctx.run()
+    target = ctx.image_products().image_I.copy()
+    ctx.set_cell_multipliers(None, None)
+    fwd_ms = adj_ms = 0.0
+    st = None
+    for it in range(args.warmup + args.steps):
+        ctx.init_image_forward_photons(p.image_nx, p.image_ny, workloads.C4_BACK_DISTANCE)
+        st, f_ms = timed_call(stream, lambda: ctx.forward_checkpointed(workloads.C4_CHECKPOINT_INTERVAL))
+        img = ctx.image_products().image_I
+        dL = 2.0 * (img - target)
+        (ga, ge), a_ms = timed_call(stream, lambda: ctx.adjoint_image_I(dL, shape))
+        if it >= args.warmup:
+            fwd_ms += f_ms
+            adj_ms += a_ms
+    ctx.close()
+    n = p.image_nx * p.image_ny
+    total = fwd_ms + adj_ms
+    print(json.dumps({
+        "metric": "adjoint (checkpointed forward + reverse sweep) rays/s on 1 B200", "value": n * args.steps / (total * 1e-3),
+        "unit": "rays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total / args.steps, "forward_ms": fwd_ms / args.steps, "adjoint_ms": adj_ms / args.steps,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic (Fishbone-Moncrief torus, seeded lognormal target)",
+        "photon_calls": st["photon_calls"], "nonzero_gradient_cells": int(np.count_nonzero(ga) + np.count_nonzero(ge)),
+        "config": {"workload": w.name, "pixels": f"{p.image_nx}x{p.image_ny}", "grid": "x".join(map(str, w.grid)),
+                   "checkpoint_interval": workloads.C4_CHECKPOINT_INTERVAL}}), flush=True)
+
+
+def run_disk(args):
+    """C5: disk-mode scattering Monte Carlo -- about 1e7 packets emitted on the
+    device from the 128x64x64 torus, traced with isotropic fluid-frame
+    scattering to escape or capture.  One step = emission + transport."""
+    import torch
+    from grt import lib, workloads
+    dist_setup(args.gpus)
+    w = workloads.C5
+    p = w.params()
+    stream = torch.cuda.Stream()
+    ctx = lib.Context(p)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload_grid(w.torus())
+    init_ms = run_ms = 0.0
+    st = None
+    n = 0
+    for it in range(args.warmup + args.steps):
+        n, i_ms = timed_call(stream, ctx.init_disk_photons)
+        if it == 0:
+            q = p.copy()
+            q.nphotons = n
+            ctx.set_params(q)
+        st, r_ms = timed_call(stream, ctx.run)
+        if it >= args.warmup:
+            init_ms += i_ms
+            run_ms += r_ms
+    ctx.close()
+    total = init_ms + run_ms
+    print(json.dumps({
+        "metric": "disk-mode packets/s on 1 B200 (emission + scattering transport)", "value": n * args.steps / (total * 1e-3),
+        "unit": "packets/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
+        "emission_ms": init_ms / args.steps, "transport_ms": run_ms / args.steps,
+        "rk_steps_per_s": st["accepted_steps"] * args.steps / (total * 1e-3), "packets": n,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic (Fishbone-Moncrief torus)",
+        "config": {"workload": w.name, "grid": "x".join(map(str, w.grid)), "spin": w.spin}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--workload", default="c2", choices=("c1", "c2", "c3", "c4", "c5"),
+                    help="c2 (the headline), c1, c3 (the 64-image batch), c4 (adjoint), c5 (disk mode)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="use the library's default launch shape")
     ap.add_argument("--forms", default="fp64,fp64_batched,mixed_batched",
@@ -553,6 +649,10 @@ def main():
     args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c4":
+        run_adjoint(args)
+    elif args.workload == "c5":
+        run_disk(args)
     else:
         run_ours(args)
 

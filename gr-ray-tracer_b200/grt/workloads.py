@@ -185,8 +185,11 @@ class DiskWorkload:
 C5 = DiskWorkload("c5_disk_1e7", (128, 64, 64), 0.9, 210.0)
 
 
-WORKLOADS = {"c1": C1, "c2": C2}
-BATCHES = {"c2": C2_BATCH, "c3": C3}
+# single-image workload of each key (for c3, the batch's base image: 256x256 at 60 deg)
+WORKLOADS = {"c1": C1, "c2": C2, "c3": C3.base}
+# the C1 image at the four frequency channels (for the batched forms of --workload c1)
+C1_BATCH = BatchWorkload("c1_rk4_64px_x4freq", C1, [(C1.inclination_deg, C1.pixels, f) for f in FREQ_CHANNELS_GHZ])
+BATCHES = {"c1": C1_BATCH, "c2": C2_BATCH, "c3": C3}
 
 
 def scaled(w: ImageWorkload, pixels=None, grid=None, **extra) -> ImageWorkload:
