@@ -82,6 +82,7 @@ struct Lane {
     int zero_all;         // a shared event zeroed every channel's Stokes vector
     long long pix;
     int fast;             // precision hint of the current call (mixed form)
+    int gen_pending;      // backward-leg launch: stopped at first fluid contact, generation left to leg 2
     int need_k1;          // the call's k1 = f(state) is still to be evaluated
     double dl_try;
     V7 k1;
@@ -99,6 +100,7 @@ GRT_DEV void load_photon(const KPhotons& P, long long i, Lane& L) {
     L.calls = 0;
     L.have_radius = 0;
     L.mid_call = 0;
+    L.gen_pending = 0;
 }
 
 GRT_DEV void store_photon(const KPhotons& P, const Lane& L, int terminated, double tdisp, double pdisp,
@@ -354,6 +356,81 @@ GRT_DEV bool generate_packet(const KParams& kp, const FluidSample& fs, uint64_t 
     return false;
 }
 
+// The first fluid contact of an image-backward ray (integrate_cart_ks.hpp:
+// 351-363): the cell's packet count and the generator give the packet's
+// frequency and energy; the ray reverses (dlambda negated) into ImageForward,
+// or is Rejected when no packet is generated.  SHARE: every other channel of
+// the geodesic draws with its own id and frequency; a channel rejected on its
+// own is written out (counted in *ch_term), and if the lead is rejected
+// another channel is promoted.  `step` is the global index of the call.
+// Returns 1 if the ray terminated.
+template <bool SHARE>
+GRT_DEV int generate_at_contact(const KParams& kp, Lane& L, const FluidSample& fs, int64_t step, int* ch_term) {
+    const KImage& im = image_params(kp, L.img);
+    int terminated = 0;
+    double nu = 0.0, E = 0.0;
+    const double dcode = fs.fluid.density_g_cm3 / kp.density_scale;
+    const int packets = ComputeSuperphotonsPerCell(dcode, kp.norm);
+    bool generated = generate_packet(kp, fs, L.id, step, packets, im.nu_custom, nu, E);
+    if (SHARE) {
+        // every other channel draws with its own id and frequency
+        int promote = -1;
+        for (int c = 0; c < L.nchan; ++c) {
+            if (c == L.lead || ((L.done >> c) & 1u)) continue;
+            const long long sc = chan_slot(kp, L.grp, c, L.pix);
+            double nu_c = 0.0, E_c = 0.0;
+            const double f_c = image_params(kp, chan_image(kp, L.grp, c)).nu_custom;
+            if (generate_packet(kp, fs, kp.ph.id[sc], step, packets, f_c, nu_c, E_c)) {
+                kp.ph.frequency[sc] = nu_c;
+                kp.ph.I[sc] = E_c;
+                kp.ph.Q[sc] = 0.0;
+                kp.ph.U[sc] = 0.0;
+                kp.ph.V[sc] = 0.0;
+                if (!generated && promote < 0) promote = c;
+            } else {
+                // rejected on its own: the state after this step, Stokes zeroed
+                store_follower(kp.ph, L, sc, 1, 4, 0.0, 0.0, 0, 1, L.dl);
+                L.done |= 1u << c;
+                ++*ch_term;
+            }
+        }
+        if (!generated && promote >= 0) {
+            // the lead is rejected on its own; channel `promote` carries on
+            L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+            const int ph_keep = L.phase;
+            L.phase = 4;
+            store_photon(kp.ph, L, 1, 0.0, 0.0, 0);
+            L.phase = ph_keep;
+            L.done |= 1u << L.lead;
+            ++*ch_term;
+            const long long sc = chan_slot(kp, L.grp, promote, L.pix);
+            L.lead = promote;
+            L.idx = sc;
+            L.id = kp.ph.id[sc];
+            L.img = chan_image(kp, L.grp, promote);
+            nu = kp.ph.frequency[sc];
+            E = kp.ph.I[sc];
+            generated = true;
+        }
+    }
+    if (generated) {
+        L.freq = nu;
+        double ee = 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ee -= L.s[4 + c] * fs.e[0][c];
+        L.emit = ee;
+        L.I[0] = E;
+        L.I[1] = L.I[2] = L.I[3] = 0.0;
+        L.dl = -fabs(L.dl);
+        L.phase = 2;  // ImageForward
+    } else {
+        L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
+        L.phase = 4;  // Rejected
+        terminated = 1;
+    }
+    return terminated;
+}
+
 // SHARE: the lane also carries the other channels of its group (their
 // frequencies and Stokes vectors in their photon slots); *ch_term counts the
 // channels that terminated on their own in this call.
@@ -371,65 +448,12 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
     const bool sampled = needs && sample_fluid<RAW>(kp, ax, L.s, L.radius, fs);
     int terminated = 0;
     if (LEG != 2 && kp.image_mode && backward && sampled) {
-        double nu = 0.0, E = 0.0;
-        const double dcode = fs.fluid.density_g_cm3 / kp.density_scale;
-        const int packets = ComputeSuperphotonsPerCell(dcode, kp.norm);
-        bool generated = generate_packet(kp, fs, L.id, step, packets, im.nu_custom, nu, E);
-        if (SHARE) {
-            // every other channel draws with its own id and frequency
-            int promote = -1;
-            for (int c = 0; c < L.nchan; ++c) {
-                if (c == L.lead || ((L.done >> c) & 1u)) continue;
-                const long long sc = chan_slot(kp, L.grp, c, L.pix);
-                double nu_c = 0.0, E_c = 0.0;
-                const double f_c = image_params(kp, chan_image(kp, L.grp, c)).nu_custom;
-                if (generate_packet(kp, fs, kp.ph.id[sc], step, packets, f_c, nu_c, E_c)) {
-                    kp.ph.frequency[sc] = nu_c;
-                    kp.ph.I[sc] = E_c;
-                    kp.ph.Q[sc] = 0.0;
-                    kp.ph.U[sc] = 0.0;
-                    kp.ph.V[sc] = 0.0;
-                    if (!generated && promote < 0) promote = c;
-                } else {
-                    // rejected on its own: the state after this step, Stokes zeroed
-                    store_follower(kp.ph, L, sc, 1, 4, 0.0, 0.0, 0, 1, L.dl);
-                    L.done |= 1u << c;
-                    ++*ch_term;
-                }
-            }
-            if (!generated && promote >= 0) {
-                // the lead is rejected on its own; channel `promote` carries on
-                L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
-                const int ph_keep = L.phase;
-                L.phase = 4;
-                store_photon(kp.ph, L, 1, 0.0, 0.0, 0);
-                L.phase = ph_keep;
-                L.done |= 1u << L.lead;
-                ++*ch_term;
-                const long long sc = chan_slot(kp, L.grp, promote, L.pix);
-                L.lead = promote;
-                L.idx = sc;
-                L.id = kp.ph.id[sc];
-                L.img = chan_image(kp, L.grp, promote);
-                nu = kp.ph.frequency[sc];
-                E = kp.ph.I[sc];
-                generated = true;
-            }
-        }
-        if (generated) {
-            L.freq = nu;
-            double ee = 0.0;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) ee -= L.s[4 + c] * fs.e[0][c];
-            L.emit = ee;
-            L.I[0] = E;
-            L.I[1] = L.I[2] = L.I[3] = 0.0;
-            L.dl = -fabs(L.dl);
-            L.phase = 2;  // ImageForward
+        if (LEG == 1) {
+            // the backward-leg launch stops here: the forward-leg launch
+            // samples this position again and generates (one call, split)
+            L.gen_pending = 1;
         } else {
-            L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
-            L.phase = 4;  // Rejected
-            terminated = 1;
+            terminated = generate_at_contact<SHARE>(kp, L, fs, step, ch_term);
         }
     } else if (LEG != 1 && sampled && !backward) {
         const double I_before = L.I[0];
@@ -527,9 +551,11 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
 // State of a live photon that the next launch over the queue needs besides
 // its photon slot: the calls taken (backward leg to forward leg) and, when
 // channels share the geodesic, which channel leads and which finished.
+// A photon the backward-leg launch stopped at its first fluid contact is
+// carried as -(calls + 1).
 template <bool SHARE, int LEG>
 GRT_DEV void store_carry(const KParams& kp, const Lane& L) {
-    if (LEG == 1) kp.calls_carry[L.q] = L.calls;
+    if (LEG == 1) kp.calls_carry[L.q] = L.gen_pending ? -(L.calls + 1) : L.calls;
     if (SHARE && kp.share_state)
         kp.share_state[L.q] = (static_cast<unsigned long long>(L.lead) << 32) | L.done;
 }
@@ -538,10 +564,12 @@ GRT_DEV void store_carry(const KParams& kp, const Lane& L) {
 // LEG splits an image-mode launch into two launches over the same queue:
 //   0  whole rays (disk mode, or image mode in one launch);
 //   1  the backward leg: photons in ImageBackward only; a lane hands its
-//      photon over when a call leaves it in another phase (after generation)
-//      -- stored like a budget end, with the calls taken so far in
-//      KParams::calls_carry[q];
-//   2  everything after: photons in any live phase but ImageBackward, resuming
+//      photon over at its first fluid contact, before the packet generation
+//      of that call -- stored like a budget end, with the calls taken so far
+//      in KParams::calls_carry[q] (negated: -(calls + 1), generation pending);
+//   2  everything after: photons in any live phase but ImageBackward, and
+//      ImageBackward photons with a generation pending, which first finish
+//      that call (sample the same position again, generate); they resume
 //      with the calls the backward launch left in calls_carry[q].
 // Each photon takes the same calls in the same order either way, so the two
 // launches give the one-launch result bit for bit; each loop body holds only
@@ -612,12 +640,17 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                         L.zero_all = 0;
                         slot = chan_slot(kp, lo, L.lead, L.pix);
                     }
+                    const long long carry = (LEG == 2 && q >= 0) ? kp.calls_carry[q] : 0;
                     if (q >= 0 && !kp.ph.terminate[slot] &&
-                        (LEG == 0 || ((kp.ph.phase[slot] == 1) == (LEG == 1)))) {
+                        (LEG == 0 || (LEG == 1 && kp.ph.phase[slot] == 1) ||
+                         (LEG == 2 && (kp.ph.phase[slot] != 1 || carry < 0)))) {
                         load_photon(kp.ph, slot, L);
                         L.idx = slot;
                         L.q = q;
-                        if (LEG == 2) L.calls = kp.calls_carry[q];
+                        if (LEG == 2) {
+                            L.calls = carry < 0 ? -carry - 1 : carry;
+                            L.gen_pending = carry < 0 ? 1 : 0;
+                        }
                         L.img = SHARE ? chan_image(kp, L.grp, L.lead) : image_of_photon(kp, q);
                         have_disp = 0;
                     }
@@ -637,6 +670,24 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
 
         // ---- one unit of work for this lane ----
         int finished = 0, terminated = 0;
+        if (LEG == 2 && L.gen_pending) {
+            // the rest of the call that reached the first fluid contact in
+            // the backward-leg launch: the same position samples the same
+            // cell, then the packet is generated
+            L.gen_pending = 0;
+            L.radius = ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
+            L.have_radius = 1;
+            FluidSample fs;
+            int ch_term = 0;
+            if (sample_fluid<RAW>(kp, ax, L.s, L.radius, fs))
+                terminated = generate_at_contact<SHARE>(kp, L, fs, kp.step0 + L.calls - 1, &ch_term);
+            if (SHARE && ch_term) {
+                cnt.terminated += ch_term;
+                const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
+                if (ts > cnt.max_term_step) cnt.max_term_step = ts;
+            }
+            finished = terminated;
+        } else {
         if (!L.mid_call) {
             if (L.calls >= kp.budget) {
                 finished = 1;  // budget of this launch used; photon stays live
@@ -667,7 +718,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                         const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
                         if (ts > cnt.max_term_step) cnt.max_term_step = ts;
                     }
-                    finished = terminated || (LEG == 1 && L.phase != 1);
+                    finished = terminated || (LEG == 1 && (L.phase != 1 || L.gen_pending));
                 } else {
                     // Mixed form: an RK45 call may use the FP32 right-hand side only
                     // when its step sequence cannot change which fluid cell the ray
@@ -702,7 +753,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                     const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
                     if (ts > cnt.max_term_step) cnt.max_term_step = ts;
                 }
-                finished = terminated || (LEG == 1 && L.phase != 1);
+                finished = terminated || (LEG == 1 && (L.phase != 1 || L.gen_pending));
             } else {
                 ++cnt.rejected;
                 if (L.attempts >= 12) {
@@ -712,6 +763,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                 }
             }
         }
+        }  // one call, or one RK45 attempt
         if (finished) {
             const int stored = store_all<SHARE>(kp, L, terminated, tdisp, pdisp, have_disp);
             if (terminated) {
