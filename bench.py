@@ -180,20 +180,13 @@ def barrier(world):
 
 
 def pinned_photons(n):
-    """Photon SoA whose arrays live in pinned (page-locked) host memory."""
-    import numpy as np
+    """Photon SoA in one pinned (page-locked) host block laid out like the
+    library's device block (grt_host_photon_layout), so it moves in one copy."""
     import torch
-    from grt.abi import PHOTON_FIELDS, PhotonArrays
-    pa = PhotonArrays(0)
-    pa.n = n
-    keep = []
-    for f in PHOTON_FIELDS:
-        dt = {"id": torch.int64, "terminate": torch.uint8, "phase": torch.uint8}.get(f, torch.float64)
-        t = torch.empty(n, dtype=dt, pin_memory=True)
-        keep.append(t)
-        arr = t.numpy()
-        setattr(pa, f, arr.view(np.uint64) if f == "id" else arr)
-    pa._keep = keep
+    from grt.abi import PhotonArrays
+    t = torch.empty(146 * n, dtype=torch.uint8, pin_memory=True)
+    pa = PhotonArrays.block(n, t.numpy())
+    pa._keep = t
     return pa
 
 

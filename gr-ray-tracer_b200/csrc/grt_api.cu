@@ -49,23 +49,44 @@ struct DevBuf {
     }
 };
 
+template <class T>
+struct FieldView {
+    T* ptr = nullptr;
+};
+
+// Byte offset of photon field k (grt_photon_soa order: 0 id, 1..17 the
+// doubles, 18 terminate, 19 phase) in a block of n photons: the fields back
+// to back, 146 bytes per photon, the 8-byte fields first.
+size_t photon_field_offset(size_t n, int k) { return k <= 17 ? 8 * n * static_cast<size_t>(k) : 144 * n + n * (k - 18); }
+
+// The photon SoA in one device block laid out by photon_field_offset; a host
+// SoA in the same layout (grt_host_photon_layout) moves with one copy.
 struct PhotonBufs {
-    DevBuf<uint64_t> id;
-    DevBuf<double> f[17];  // frequency .. phi_disp in grt_photon_soa order
-    DevBuf<uint8_t> term, phase;
-    cudaError_t alloc(size_t n) {
-        cudaError_t e = id.alloc(n);
-        for (auto& b : f)
-            if (e == cudaSuccess) e = b.alloc(n);
-        if (e == cudaSuccess) e = term.alloc(n);
-        if (e == cudaSuccess) e = phase.alloc(n);
-        return e;
+    DevBuf<unsigned char> block;
+    size_t n = 0;
+    FieldView<uint64_t> id;
+    FieldView<double> f[17];  // frequency .. phi_disp in grt_photon_soa order
+    FieldView<uint8_t> term, phase;
+    cudaError_t alloc(size_t count) {
+        const cudaError_t e = block.alloc(146 * count);
+        if (e != cudaSuccess) {
+            release();
+            return e;
+        }
+        n = count;
+        unsigned char* b = block.ptr;
+        id.ptr = reinterpret_cast<uint64_t*>(b);
+        for (int q = 0; q < 17; ++q) f[q].ptr = reinterpret_cast<double*>(b + photon_field_offset(count, q + 1));
+        term.ptr = b + photon_field_offset(count, 18);
+        phase.ptr = b + photon_field_offset(count, 19);
+        return cudaSuccess;
     }
     void release() {
-        id.release();
-        for (auto& b : f) b.release();
-        term.release();
-        phase.release();
+        block.release();
+        n = 0;
+        id.ptr = nullptr;
+        for (auto& v : f) v.ptr = nullptr;
+        term.ptr = phase.ptr = nullptr;
     }
     grt::KPhotons view() const {
         grt::KPhotons k;
@@ -86,6 +107,18 @@ double* const* soa_doubles(const grt_photon_soa* s, double* out[17]) {
                        s->dlambda, s->theta_disp, s->phi_disp};
     for (int q = 0; q < 17; ++q) out[q] = src[q];
     return out;
+}
+
+// True when the 20 fields of s are one block in photon_field_offset's layout
+// for n photons (the layout grt_host_photon_layout hands out).
+bool soa_is_block(const grt_photon_soa* s, size_t n) {
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(s->id);
+    if (!b) return false;
+    double* d[17];
+    soa_doubles(s, d);
+    for (int q = 0; q < 17; ++q)
+        if (reinterpret_cast<const unsigned char*>(d[q]) != b + photon_field_offset(n, q + 1)) return false;
+    return s->terminate == b + photon_field_offset(n, 18) && s->phase == b + photon_field_offset(n, 19);
 }
 
 }  // namespace
@@ -608,11 +641,17 @@ grt_status grt_upload_photons(grt_ctx* c, const grt_photon_soa* s, size_t n) {
     if (!s->id || !s->terminate || !s->phase) return fail(c, GRT_EINVAL, "null photon field");
     for (double* q : src)
         if (!q) return fail(c, GRT_EINVAL, "null photon field");
-    GRT_CUDA(c, cudaMemcpyAsync(c->ph.id.ptr, s->id, n * 8, cudaMemcpyHostToDevice, c->stream), "H2D id");
-    for (int q = 0; q < 17; ++q)
-        GRT_CUDA(c, cudaMemcpyAsync(c->ph.f[q].ptr, src[q], n * 8, cudaMemcpyHostToDevice, c->stream), "H2D photons");
-    GRT_CUDA(c, cudaMemcpyAsync(c->ph.term.ptr, s->terminate, n, cudaMemcpyHostToDevice, c->stream), "H2D term");
-    GRT_CUDA(c, cudaMemcpyAsync(c->ph.phase.ptr, s->phase, n, cudaMemcpyHostToDevice, c->stream), "H2D phase");
+    if (soa_is_block(s, n)) {
+        // the host block has the device block's layout: one transfer
+        GRT_CUDA(c, cudaMemcpyAsync(c->ph.block.ptr, s->id, 146 * n, cudaMemcpyHostToDevice, c->stream), "H2D photons");
+    } else {
+        GRT_CUDA(c, cudaMemcpyAsync(c->ph.id.ptr, s->id, n * 8, cudaMemcpyHostToDevice, c->stream), "H2D id");
+        for (int q = 0; q < 17; ++q)
+            GRT_CUDA(c, cudaMemcpyAsync(c->ph.f[q].ptr, src[q], n * 8, cudaMemcpyHostToDevice, c->stream),
+                     "H2D photons");
+        GRT_CUDA(c, cudaMemcpyAsync(c->ph.term.ptr, s->terminate, n, cudaMemcpyHostToDevice, c->stream), "H2D term");
+        GRT_CUDA(c, cudaMemcpyAsync(c->ph.phase.ptr, s->phase, n, cudaMemcpyHostToDevice, c->stream), "H2D phase");
+    }
     if (keep_images && c->batched && c->groups_share && c->geodesics)
         GRT_CUDA(c, cudaMemsetAsync(c->share_state.ptr, 0, c->geodesics * sizeof(unsigned long long), c->stream),
                  "memset share state");
@@ -621,12 +660,33 @@ grt_status grt_upload_photons(grt_ctx* c, const grt_photon_soa* s, size_t n) {
 
 size_t grt_photon_count(const grt_ctx* c) { return c ? c->n : 0; }
 
+size_t grt_photon_block_bytes(size_t n) { return 146 * n; }
+
+grt_status grt_host_photon_layout(void* block, size_t n, grt_photon_soa* soa) {
+    if (!soa || (!block && n)) return GRT_EINVAL;
+    if (reinterpret_cast<uintptr_t>(block) % 8 != 0) return GRT_EINVAL;
+    unsigned char* b = static_cast<unsigned char*>(block);
+    soa->id = reinterpret_cast<uint64_t*>(b);
+    double** d[17] = {&soa->frequency, &soa->emission_frame_energy, &soa->x0, &soa->x1, &soa->x2, &soa->x3,
+                      &soa->k0, &soa->k1, &soa->k2, &soa->k3, &soa->I, &soa->Q, &soa->U, &soa->V,
+                      &soa->dlambda, &soa->theta_disp, &soa->phi_disp};
+    for (int q = 0; q < 17; ++q) *d[q] = reinterpret_cast<double*>(b + photon_field_offset(n, q + 1));
+    soa->terminate = b + photon_field_offset(n, 18);
+    soa->phase = b + photon_field_offset(n, 19);
+    return GRT_OK;
+}
+
 grt_status grt_download_photons(grt_ctx* c, grt_photon_soa* s) {
     if (!c || !s) return GRT_EINVAL;
     const size_t n = c->n;
     if (n == 0) return GRT_OK;
     double* dst[17];
     soa_doubles(s, dst);
+    if (soa_is_block(s, n)) {
+        GRT_CUDA(c, cudaMemcpyAsync(s->id, c->ph.block.ptr, 146 * n, cudaMemcpyDeviceToHost, c->stream), "D2H");
+        GRT_CUDA(c, cudaStreamSynchronize(c->stream), "sync");
+        return GRT_OK;
+    }
     if (s->id) GRT_CUDA(c, cudaMemcpyAsync(s->id, c->ph.id.ptr, n * 8, cudaMemcpyDeviceToHost, c->stream), "D2H");
     for (int q = 0; q < 17; ++q)
         if (dst[q]) GRT_CUDA(c, cudaMemcpyAsync(dst[q], c->ph.f[q].ptr, n * 8, cudaMemcpyDeviceToHost, c->stream), "D2H");

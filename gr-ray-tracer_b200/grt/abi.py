@@ -140,6 +140,25 @@ class PhotonArrays:
             setattr(self, f, np.zeros(self.n, dtype=PHOTON_DTYPES.get(f, np.float64)))
 
     @classmethod
+    def block(cls, n: int, buffer=None):
+        """The SoA as views into one byte buffer of 146 n bytes in the layout of
+        grt_host_photon_layout (id, the 17 doubles, terminate, phase back to
+        back), which grt_upload_photons / grt_download_photons move with one
+        transfer.  `buffer` (e.g. a pinned tensor's numpy view) or a new array."""
+        n = int(n)
+        buf = np.zeros(146 * n, dtype=np.uint8) if buffer is None else buffer
+        if buf.size < 146 * n or buf.ctypes.data % 8:
+            raise ValueError("the buffer needs 146 * n bytes, 8-byte aligned")
+        pa = cls.__new__(cls)
+        pa.n = n
+        pa._buffer = buf
+        for k, f in enumerate(PHOTON_FIELDS):
+            off = 8 * n * k if k <= 17 else 144 * n + n * (k - 18)
+            size = 8 if k <= 17 else 1
+            setattr(pa, f, buf[off:off + size * n].view(PHOTON_DTYPES.get(f, np.float64)))
+        return pa
+
+    @classmethod
     def from_dict(cls, d):
         n = len(d["x0"])
         pa = cls(n)

@@ -99,6 +99,10 @@ def load(path: Path | None = None):
                                                C.c_size_t]
     L.grt_write_output_step_npz.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int64, C.c_int32, C.c_char_p, C.c_uint64]
     L.grt_run_with_output.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64, P(RunStats)]
+    L.grt_photon_block_bytes.argtypes = [C.c_size_t]
+    L.grt_photon_block_bytes.restype = C.c_size_t
+    L.grt_host_photon_layout.argtypes = [vp, C.c_size_t, P(PhotonSoA)]
+    L.grt_host_photon_layout.restype = C.c_int
     for name in ("grt_parse_output_variables", "grt_output_options_from_toml", "grt_write_output_step_npz",
                  "grt_run_with_output", "grt_set_cell_multipliers", "grt_forward_checkpointed", "grt_adjoint_image_I",
                  "grt_init_image_batch", "grt_get_batch_image_products", "grt_write_batch_products_npz",

@@ -271,6 +271,19 @@ grt_status grt_download_photons(grt_ctx* ctx, grt_photon_soa* soa);
 size_t grt_photon_count(const grt_ctx* ctx);
 
 /*
+ * Host photon block (no counterpart in the reference, whose Photons are 20
+ * separate Kokkos views): the device keeps the SoA in one block, the 20
+ * fields back to back in grt_photon_soa order (id, the 17 doubles, terminate,
+ * phase; 146 bytes per photon).  grt_host_photon_layout points soa's fields
+ * into a caller-owned host block of grt_photon_block_bytes(n) bytes
+ * (8-byte aligned; pinned memory for asynchronous copies) in that layout;
+ * grt_upload_photons / grt_download_photons given such a SoA move it with
+ * one transfer instead of 20.
+ */
+size_t grt_photon_block_bytes(size_t n);
+grt_status grt_host_photon_layout(void* block, size_t n, grt_photon_soa* soa);
+
+/*
  * Image products of the ImageArrived photons, accumulated on the device
  * (build_observation_products, observation.hpp:31-84): every output array is
  * a caller-owned host buffer sized from p.image_nx/ny/spectrum_bins.

@@ -121,3 +121,27 @@ def test_param_validation():
     p.camera_distance = -1.0
     with pytest.raises(lib.GrtError, match="camera distance"):
         lib.validate_params(p)
+
+
+def test_host_photon_block_layout_matches_the_library():
+    """abi.PhotonArrays.block lays the 20 fields out exactly where
+    grt_host_photon_layout points them (the layout that moves in one copy)."""
+    import ctypes as C
+
+    import numpy as np
+
+    from grt import abi, lib
+    L = lib.load()
+    for n in (0, 1, 7, 1000):
+        assert L.grt_photon_block_bytes(n) == 146 * n
+        pa = abi.PhotonArrays.block(n)
+        soa = abi.PhotonSoA()
+        assert L.grt_host_photon_layout(C.c_void_p(pa._buffer.ctypes.data), n, C.byref(soa)) == 0
+        mine = pa.soa()
+        for f in abi.PHOTON_FIELDS:
+            a = C.cast(getattr(soa, f), C.c_void_p).value
+            b = C.cast(getattr(mine, f), C.c_void_p).value
+            assert a == b, (n, f)
+        if n:
+            pa.x0[:] = np.arange(n)
+            assert np.array_equal(pa.x0, np.arange(n)) and not pa.x1.any()

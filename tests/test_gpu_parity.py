@@ -136,3 +136,31 @@ def test_mixed_precision_image_error(gpu, oracle, w):
     got, gprod, _ = run_gpu(gpu, pm, grid, nx=w.pixels, ny=w.pixels)
     err = stokes_l2_rel(gprod.image_I, rprod.image_I)
     assert err <= 1e-5, err
+
+
+def test_host_photon_block_moves_in_one_copy(gpu):
+    # a host SoA in the library's block layout (one transfer each way) and a
+    # SoA of separate arrays (one transfer per field) carry the same photons
+    w = C2_MINI
+    p = w.params()
+    grid = w.torus()
+    outs = []
+    for block in (True, False):
+        ctx = gpu.Context(p)
+        try:
+            ctx.upload_grid(grid)
+            ctx.init_image_photons(w.pixels, w.pixels)
+            n = ctx.n
+            host = abi.PhotonArrays.block(n) if block else abi.PhotonArrays(n)
+            ctx.download_photons(host)
+            host.terminate[::5] = 1
+            ctx.upload_photons(host)
+            ctx.run()
+            out = abi.PhotonArrays.block(n) if block else abi.PhotonArrays(n)
+            ctx.download_photons(out)
+        finally:
+            ctx.close()
+        outs.append(out)
+    for f in abi.PHOTON_FIELDS:
+        assert np.array_equal(getattr(outs[0], f), getattr(outs[1], f)), f
+    assert outs[0].terminate.all()
