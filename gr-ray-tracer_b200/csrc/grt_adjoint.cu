@@ -80,7 +80,7 @@ GRT_DEV int run_call(const KParams& kp, const Axes& ax, const KStore& kk, Lane& 
     L.dl_try = L.dl;
     for (int attempt = 0; attempt < 12; ++attempt) {
         const double taken = L.dl_try;
-        if (rk45_attempt<Fp64Rhs>(kp, L.s, &L.dl_try, L.k1, attempt == 0, 0, kk)) {
+        if (rk45_attempt<Fp64Rhs>(kp, L.s, &L.dl_try, attempt == 0, 0, kk)) {
             L.dl = L.dl_try;
             const int phase0 = L.phase;
             return post_step<false, Rec>(kp, ax, L, phase0, taken, step, tdisp, pdisp, have_disp, rec);

@@ -127,10 +127,10 @@ inline KImage make_kimage(double theta, double phi, double distance, double widt
     return im;
 }
 
-// Dynamic shared memory of a trace launch: k2..k5 slots for RK45 (4*7 doubles
+// Dynamic shared memory of a trace launch: k1..k5 slots for RK45 (5*7 doubles
 // per thread) plus the separable axes and their half-spans (2*(nr+nth+nph)).
 inline size_t dev_trace_smem_bytes(int integrator, int threads, bool separable, int nr, int nth, int nph) {
-    size_t n = integrator == 1 ? static_cast<size_t>(4 * 7) * threads : 0;
+    size_t n = integrator == 1 ? static_cast<size_t>(5 * 7) * threads : 0;
     if (separable) n += 2 * static_cast<size_t>(nr + nth + nph);
     return n * sizeof(double);
 }

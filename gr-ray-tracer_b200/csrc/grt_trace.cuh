@@ -85,7 +85,6 @@ struct Lane {
     int gen_pending;      // backward-leg launch: stopped at first fluid contact, generation left to leg 2
     int need_k1;          // the call's k1 = f(state) is still to be evaluated
     double dl_try;
-    V7 k1;
 };
 
 GRT_DEV void load_photon(const KPhotons& P, long long i, Lane& L) {
@@ -210,9 +209,11 @@ static __constant__ double kFehlbergA[5][5] = {
 // __launch_bounds__ use the same constant).
 constexpr int kTraceThreads = 128;
 
-// Per-thread slots for k2..k5 in shared memory: [4][7][kTraceThreads] doubles,
-// thread-contiguous so a warp's accesses are conflict-free; base already
-// points at this thread's column, so a slot is a constant offset from it.
+// Per-thread slots for the stage derivatives k1..k5 in shared memory:
+// [5][7][kTraceThreads] doubles, thread-contiguous so a warp's accesses are
+// conflict-free; base already points at this thread's column, so a slot is a
+// constant offset from it.  k1 stays there across the retries of one call.
+constexpr int kStageSlots = 5;
 struct KStore {
     double* base;
     GRT_DEV double& at(int j, int c) const { return base[(j * 7 + c) * kTraceThreads]; }
@@ -227,13 +228,12 @@ static __device__ __noinline__ double controller_root(double x) { return fourth_
 // if accepted (s advanced), 0 if rejected; *dl receives the next proposed step
 // either way.  All right-hand sides go through one site in a rolled stage
 // loop -- a lane that needs k1 runs it one iteration ahead of the others, so
-// the warp stays converged on the same code -- and k2..k5 live in shared
-// memory.  Each stage input is summed over j = 1..t-1 left to right, the
+// the warp stays converged on the same code -- and k1..k5 live in shared
+// memory (slots 0..4), which keeps registers for the right-hand side.  Each stage input is summed over j = 1..t-1 left to right, the
 // reference's association; for the first stage, dt*(a21 k1) equals the
 // reference's (dt*a21)*k1 because a21 = 1/4 is a power of two.
 template <class RHS>
-GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, V7& k1, int need_k1, int fast,
-                         const KStore& kk) {
+GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, int need_k1, int fast, const KStore& kk) {
     const double dt = *dl;
     V7 k6;
     double t[8];
@@ -247,24 +247,22 @@ GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, V7& k1, int
             double acc[7];
             const double a0 = kFehlbergA[st][0];
 #pragma unroll
-            for (int c = 0; c < 7; ++c) acc[c] = a0 * k1.v[c];
+            for (int c = 0; c < 7; ++c) acc[c] = a0 * kk.at(0, c);
 #pragma unroll
             for (int j = 1; j <= 4; ++j) {
                 if (j <= st) {
                     const double aj = kFehlbergA[st][j];
 #pragma unroll
-                    for (int c = 0; c < 7; ++c) acc[c] = acc[c] + aj * kk.at(j - 1, c);
+                    for (int c = 0; c < 7; ++c) acc[c] = acc[c] + aj * kk.at(j, c);
                 }
             }
 #pragma unroll
             for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + dt * acc[c];
         }
         const V7 k = RHS::eval(t, kp, fast);
-        if (st < 0) {
-            k1 = k;
-        } else if (st < 4) {
+        if (st < 4) {
 #pragma unroll
-            for (int c = 0; c < 7; ++c) kk.at(st, c) = k.v[c];
+            for (int c = 0; c < 7; ++c) kk.at(st + 1, c) = k.v[c];
         } else {
             k6 = k;
         }
@@ -275,9 +273,9 @@ GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, V7& k1, int
 #pragma unroll
     for (int c = 0; c < 7; ++c) {
         const double si = s[sidx(c)];
-        const double k3 = kk.at(1, c), k4 = kk.at(2, c), k5 = kk.at(3, c);
-        const double x4 = si + dt * (b41 * k1.v[c] + b43 * k3 + b44 * k4 + b45 * k5);
-        x5[c] = si + dt * (b51 * k1.v[c] + b53 * k3 + b54 * k4 + b55 * k5 + b56 * k6.v[c]);
+        const double k1 = kk.at(0, c), k3 = kk.at(2, c), k4 = kk.at(3, c), k5 = kk.at(4, c);
+        const double x4 = si + dt * (b41 * k1 + b43 * k3 + b44 * k4 + b45 * k5);
+        x5[c] = si + dt * (b51 * k1 + b53 * k3 + b54 * k4 + b55 * k5 + b56 * k6.v[c]);
         const double sc = kp.atol + kp.rtol * fmax(fabs(x5[c]), fabs(x4));
         const double ratio = fabs(x5[c] - x4) / sc;
         if (!isfinite(x5[c]) || !isfinite(ratio)) finite = false;
@@ -736,7 +734,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
             const double taken = L.dl_try;
             // the backward leg never uses the FP32 right-hand side (a literal
             // 0 lets the compiler drop it from the backward kernel)
-            const int ok = rk45_attempt<RHS>(kp, L.s, &L.dl_try, L.k1, L.need_k1, LEG == 1 ? 0 : L.fast, kk);
+            const int ok = rk45_attempt<RHS>(kp, L.s, &L.dl_try, L.need_k1, LEG == 1 ? 0 : L.fast, kk);
             L.need_k1 = 0;
             ++L.attempts;
             if (ok) {
@@ -809,7 +807,7 @@ GRT_DEV void stage_grid(const KParams& kp, double* smem, int integrator, Axes& a
     const KGrid& G = kp.grid;
     double* p = smem;
     kk.base = p + threadIdx.x;
-    if (integrator == 1) p += 4 * 7 * kTraceThreads;
+    if (integrator == 1) p += kStageSlots * 7 * kTraceThreads;
     if (G.available && G.separable) {
         double* r = p;
         double* th = r + G.nr;
