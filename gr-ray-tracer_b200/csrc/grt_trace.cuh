@@ -87,31 +87,45 @@ struct Lane {
     double dl_try;
 };
 
+// GEO: the backward-leg launch, which neither reads nor changes a photon's
+// id, frequency, emission-frame energy, Stokes vector or screen position
+// (generation, transfer, scattering and arrival all happen in the forward-leg
+// launch): only the geodesic part is loaded and stored, and the Stokes vector
+// only zeroed, which keeps those fields out of the lane's registers.
+template <bool GEO = false>
 GRT_DEV void load_photon(const KPhotons& P, long long i, Lane& L) {
-    L.id = P.id[i];
-    L.freq = P.frequency[i];
-    L.emit = P.emission_frame_energy[i];
+    if (!GEO) {
+        L.id = P.id[i];
+        L.freq = P.frequency[i];
+        L.emit = P.emission_frame_energy[i];
+        L.I[0] = P.I[i]; L.I[1] = P.Q[i]; L.I[2] = P.U[i]; L.I[3] = P.V[i];
+    }
     L.s[0] = P.x0[i]; L.s[1] = P.x1[i]; L.s[2] = P.x2[i]; L.s[3] = P.x3[i];
     L.s[4] = P.k0[i]; L.s[5] = P.k1[i]; L.s[6] = P.k2[i]; L.s[7] = P.k3[i];
-    L.I[0] = P.I[i]; L.I[1] = P.Q[i]; L.I[2] = P.U[i]; L.I[3] = P.V[i];
     L.dl = P.dlambda[i];
     L.phase = P.phase[i];
     L.calls = 0;
     L.have_radius = 0;
     L.mid_call = 0;
     L.gen_pending = 0;
+    L.zero_all = 0;
 }
 
+template <bool GEO = false>
 GRT_DEV void store_photon(const KPhotons& P, const Lane& L, int terminated, double tdisp, double pdisp,
                           int have_disp) {
     const long long i = L.idx;
-    P.frequency[i] = L.freq;
-    P.emission_frame_energy[i] = L.emit;
+    if (!GEO) {
+        P.frequency[i] = L.freq;
+        P.emission_frame_energy[i] = L.emit;
+        P.I[i] = L.I[0]; P.Q[i] = L.I[1]; P.U[i] = L.I[2]; P.V[i] = L.I[3];
+    } else if (L.zero_all) {
+        P.I[i] = 0.0; P.Q[i] = 0.0; P.U[i] = 0.0; P.V[i] = 0.0;
+    }
     P.x0[i] = L.s[0]; P.x1[i] = L.s[1]; P.x2[i] = L.s[2]; P.x3[i] = L.s[3];
     P.k0[i] = L.s[4]; P.k1[i] = L.s[5]; P.k2[i] = L.s[6]; P.k3[i] = L.s[7];
-    P.I[i] = L.I[0]; P.Q[i] = L.I[1]; P.U[i] = L.I[2]; P.V[i] = L.I[3];
     P.dlambda[i] = L.dl;
-    if (have_disp) {
+    if (!GEO && have_disp) {
         P.theta_disp[i] = tdisp;
         P.phi_disp[i] = pdisp;
     }
@@ -127,16 +141,17 @@ GRT_DEV long long chan_slot(const KParams& kp, int grp, int c, long long pix) {
 
 // Geodesic part of the photon state of channel slot i (its id, frequency and
 // Stokes vector are its own and already in place).
+template <bool GEO = false>
 GRT_DEV void store_follower(const KPhotons& P, const Lane& L, long long i, int terminated, int phase, double tdisp,
                             double pdisp, int have_disp, int zero_stokes, double dl) {
-    P.emission_frame_energy[i] = L.emit;
+    if (!GEO) P.emission_frame_energy[i] = L.emit;
     P.x0[i] = L.s[0]; P.x1[i] = L.s[1]; P.x2[i] = L.s[2]; P.x3[i] = L.s[3];
     P.k0[i] = L.s[4]; P.k1[i] = L.s[5]; P.k2[i] = L.s[6]; P.k3[i] = L.s[7];
     if (zero_stokes) {
         P.I[i] = 0.0; P.Q[i] = 0.0; P.U[i] = 0.0; P.V[i] = 0.0;
     }
     P.dlambda[i] = dl;
-    if (have_disp) {
+    if (!GEO && have_disp) {
         P.theta_disp[i] = tdisp;
         P.phi_disp[i] = pdisp;
     }
@@ -145,16 +160,19 @@ GRT_DEV void store_follower(const KPhotons& P, const Lane& L, long long i, int t
 }
 
 // Store the lane's photon and, in a sharing launch, every channel still riding
-// on its geodesic.  Returns the number of photons stored.
-template <bool SHARE>
+// on its geodesic.  Returns the number of photons stored.  GEO (the
+// backward-leg launch, see load_photon): the geodesic part only, and no
+// followers when the ray is handed to the forward-leg launch with its
+// generation pending (that launch stores them).
+template <bool SHARE, bool GEO = false>
 GRT_DEV int store_all(const KParams& kp, const Lane& L, int terminated, double tdisp, double pdisp, int have_disp) {
-    store_photon(kp.ph, L, terminated, tdisp, pdisp, have_disp);
+    store_photon<GEO>(kp.ph, L, terminated, tdisp, pdisp, have_disp);
     int stored = 1;
-    if (SHARE) {
+    if (SHARE && !(GEO && L.gen_pending)) {
         for (int c = 0; c < L.nchan; ++c) {
             if (c == L.lead || ((L.done >> c) & 1u)) continue;
-            store_follower(kp.ph, L, chan_slot(kp, L.grp, c, L.pix), terminated, L.phase, tdisp, pdisp, have_disp,
-                           L.zero_all, L.dl);
+            store_follower<GEO>(kp.ph, L, chan_slot(kp, L.grp, c, L.pix), terminated, L.phase, tdisp, pdisp,
+                                have_disp, L.zero_all, L.dl);
             ++stored;
         }
     }
@@ -642,7 +660,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                     if (q >= 0 && !kp.ph.terminate[slot] &&
                         (LEG == 0 || (LEG == 1 && kp.ph.phase[slot] == 1) ||
                          (LEG == 2 && (kp.ph.phase[slot] != 1 || carry < 0)))) {
-                        load_photon(kp.ph, slot, L);
+                        load_photon<LEG == 1>(kp.ph, slot, L);
                         L.idx = slot;
                         L.q = q;
                         if (LEG == 2) {
@@ -763,7 +781,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
         }
         }  // one call, or one RK45 attempt
         if (finished) {
-            const int stored = store_all<SHARE>(kp, L, terminated, tdisp, pdisp, have_disp);
+            const int stored = store_all<SHARE, LEG == 1>(kp, L, terminated, tdisp, pdisp, have_disp);
             if (terminated) {
                 cnt.terminated += stored;
                 const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
@@ -777,7 +795,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
     if (timed_out) {
         // Leave every photon consistent: write back what this lane holds.
         if (L.idx >= 0) {
-            store_all<SHARE>(kp, L, 0, tdisp, pdisp, have_disp);
+            store_all<SHARE, LEG == 1>(kp, L, 0, tdisp, pdisp, have_disp);
             store_carry<SHARE, LEG>(kp, L);
         }
         if (lane == 0) atomicAdd(&kp.counters->timed_out, 1ull);
