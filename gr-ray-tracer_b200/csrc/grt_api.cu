@@ -362,6 +362,7 @@ grt::KParams make_kparams(const grt_ctx* c) {
     // never accept radii above r_reject_hi); without a grid, everywhere.
     k.fp32_min_radius_sq = c->fluid_available ? (std::isfinite(c->r_reject_hi) ? c->r_reject_hi * c->r_reject_hi : INFINITY) : 0.0;
     k.renormalize = 1;
+    k.rcp_ok = grt::rcp_params_ok(p.spin, p.mass);
     return k;
 }
 

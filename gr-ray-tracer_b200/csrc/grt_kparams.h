@@ -129,7 +129,9 @@ struct KParams {
     double fp64_axis_sin2;     // (x^2+y^2)/(x^2+y^2+z^2) below this (polar axis) uses FP64
     double fp32_min_radius_sq; // RK45 calls start r^2 above this (outside the fluid grid) for FP32
     int renormalize;           // restore g^{mu nu} p_mu p_nu = 0 in FP64 after each accepted step
-    int pad2;
+    // spin and mass inside the range where the FP64 right-hand side may use
+    // reciprocal quotients (ks_rhs_rcp): |a| = 0 or in [2^-20, 2], M in [2^-20, 2^20]
+    int rcp_ok;
 };
 
 }  // namespace grt

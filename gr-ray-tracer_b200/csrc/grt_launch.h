@@ -127,6 +127,15 @@ inline KImage make_kimage(double theta, double phi, double distance, double widt
     return im;
 }
 
+// Whether the spin a and mass M admit the reciprocal-quotient right-hand side
+// (KParams::rcp_ok): |a| = 0 or in [2^-20, 2], M in [2^-20, 2^20].
+inline int rcp_params_ok(double a, double M) {
+    const double fa = std::fabs(a);
+    const bool a_ok = fa == 0.0 || (fa >= std::ldexp(1.0, -20) && fa <= 2.0);
+    const bool m_ok = M >= std::ldexp(1.0, -20) && M <= std::ldexp(1.0, 20);
+    return a_ok && m_ok ? 1 : 0;
+}
+
 // Dynamic shared memory of a trace launch: k1..k5 slots for RK45 (5*7 doubles
 // per thread) plus the separable axes and their half-spans (2*(nr+nth+nph)).
 inline size_t dev_trace_smem_bytes(int integrator, int threads, bool separable, int nr, int nth, int nph) {

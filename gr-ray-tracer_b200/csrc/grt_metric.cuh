@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include "grt_div.cuh"
+
 namespace grt {
 namespace dev {
 
@@ -85,6 +87,82 @@ GRT_DEV Rhs7 ks_rhs(double x, double y, double z, double pt, double px, double p
     const double ldp = ((-pt + l1 * px) + l2 * py) + l3 * pz;
     const double twoH = 2.0 * H;
     Rhs7 o;
+    o.t = -pt - (-twoH) * ldp;
+    o.x = px - twoH * l1 * ldp;
+    o.y = py - twoH * l2 * ldp;
+    o.z = pz - twoH * l3 * ldp;
+    const double ldp2 = ldp * ldp;
+    const double twoHl = twoH * ldp;
+    o.px = dH0 * ldp2 + twoHl * ((dl01 * px + dl02 * py) + dl03 * pz);
+    o.py = dH1 * ldp2 + twoHl * ((dl11 * px + dl12 * py) + dl13 * pz);
+    o.pz = dH2 * ldp2 + twoHl * ((dl21 * px + dl22 * py) + dl23 * pz);
+    return o;
+}
+
+// ks_rhs with every quotient formed from the correctly rounded reciprocal of
+// its denominator (six of them: S, 2r, B, r, D, D^2) by div_by, which rounds
+// like an IEEE division while no value under- or overflows.  That holds in
+// the box this checks first: x, y, z each an exact zero or of magnitude in
+// [2^-20, 2^20], r in [2^-24, 2^20] and S in [2^-60, 2^42], with a spin of
+// magnitude 0 or in [2^-20, 2] and a mass in [2^-20, 2^20] (checked on the
+// host: rcp_ok).  Inside it every numerator, quotient and denominator stays
+// in [2^-900, 2^900]: products of at most eight factors of at least 2^-60,
+// differences of such products (zero, or at least 2^-52 of the smaller),
+// divided by at most r^8 <= 2^160.  Outside it `ok` is false and the caller
+// evaluates ks_rhs.  The expression tree is ks_rhs's, so the result equals
+// ks_rhs bit for bit.
+GRT_DEV Rhs7 ks_rhs_rcp(double x, double y, double z, double pt, double px, double py, double pz,
+                        double a, double M, bool& ok) {
+    const double rsq = x * x + y * y + z * z;
+    const double A = rsq - a * a;
+    const double S = sqrt(A * A + 4.0 * ((a * z) * (a * z)));
+    const double r = sqrt(0.5 * (A + S));
+    ok = div_zero_or_within<-20, 19>(x) && div_zero_or_within<-20, 19>(y) && div_zero_or_within<-20, 19>(z) &&
+         div_within<-24, 19>(r) && div_within<-60, 41>(S);
+    Rhs7 o{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!ok) return o;
+    const double yS = div_recip(S);
+    const double opas = 1.0 + div_by(A, S, yS);
+    const double two_r = 2.0 * r;
+    const double y2r = div_recip(two_r);
+    const double dr0 = div_by(x * opas, two_r, y2r);
+    const double dr1 = div_by(y * opas, two_r, y2r);
+    const double dr2 = div_by(z * opas + div_by(2.0 * (a * a) * z, S, yS), two_r, y2r);
+    const double B = r * r + a * a;
+    const double yB = div_recip(B);
+    const double yr = div_recip(r);
+    const double l1 = div_by(r * x + a * y, B, yB);
+    const double l2 = div_by(r * y - a * x, B, yB);
+    const double l3 = div_by(z, r, yr);
+    const double dB0 = 2.0 * r * dr0;
+    const double dB1 = 2.0 * r * dr1;
+    const double dB2 = 2.0 * r * dr2;
+    const double dl01 = div_by((dr0 * x + r) - l1 * dB0, B, yB);
+    const double dl02 = div_by((dr0 * y - a) - l2 * dB0, B, yB);
+    const double dl03 = div_by(0.0 - l3 * dr0, r, yr);
+    const double dl11 = div_by((dr1 * x + a) - l1 * dB1, B, yB);
+    const double dl12 = div_by((dr1 * y + r) - l2 * dB1, B, yB);
+    const double dl13 = div_by(0.0 - l3 * dr1, r, yr);
+    const double dl21 = div_by(dr2 * x - l1 * dB2, B, yB);
+    const double dl22 = div_by(dr2 * y - l2 * dB2, B, yB);
+    const double dl23 = div_by(1.0 - l3 * dr2, r, yr);
+    const double r2 = r * r;
+    const double r3 = r2 * r;
+    const double D = r3 * r + (a * z) * (a * z);
+    const double yD = div_recip(D);
+    const double H = div_by(M * r3, D, yD);
+    const double four_r3 = 4.0 * r3;
+    const double dD0 = four_r3 * dr0;
+    const double dD1 = four_r3 * dr1;
+    const double dD2 = four_r3 * dr2 + 2.0 * (a * a) * z;
+    const double three_r2 = 3.0 * r2;
+    const double DD = D * D;
+    const double yDD = div_recip(DD);
+    const double dH0 = div_by(M * (three_r2 * dr0 * D - r3 * dD0), DD, yDD);
+    const double dH1 = div_by(M * (three_r2 * dr1 * D - r3 * dD1), DD, yDD);
+    const double dH2 = div_by(M * (three_r2 * dr2 * D - r3 * dD2), DD, yDD);
+    const double ldp = ((-pt + l1 * px) + l2 * py) + l3 * pz;
+    const double twoH = 2.0 * H;
     o.t = -pt - (-twoH) * ldp;
     o.x = px - twoH * l1 * ldp;
     o.y = py - twoH * l2 * ldp;

@@ -203,6 +203,7 @@ extern "C" grt_status grt_trace_device_noalloc(const grt_params* p, const grt_de
     }
     kp.a = p->spin;
     kp.M = p->mass;
+    kp.rcp_ok = grt::rcp_params_ok(p->spin, p->mass);
     kp.r_min = p->r_term_min;
     kp.r_max = p->r_term_max;
     kp.atol = p->atol;

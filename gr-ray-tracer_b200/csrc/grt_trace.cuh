@@ -50,11 +50,25 @@ GRT_DEV V7 to_v7(const Rhs7& r) {
 // state index of V7 component c
 GRT_DEV constexpr int sidx(int c) { return c < 4 ? c : c + 1; }
 
-// Right-hand-side policy of the FP64 parity form.
+// ks_rhs with IEEE divisions, out of line: the right-hand side outside the
+// box of ks_rhs_rcp.
+static __device__ __noinline__ Rhs7 ks_rhs_ieee(double x, double y, double z, double pt, double px, double py,
+                                                double pz, double a, double M) {
+    return ks_rhs(x, y, z, pt, px, py, pz, a, M);
+}
+
+// Right-hand-side policy of the FP64 parity form: ks_rhs_rcp (reciprocal
+// quotients that round like IEEE divisions) inside its box, ks_rhs outside;
+// both give ks_rhs's result bit for bit.
 // `fast` is the per-call precision hint of the mixed form (ignored here).
 struct Fp64Rhs {
     static GRT_DEV V7 eval(const double s[8], const KParams& kp, int /*fast*/) {
-        return to_v7(ks_rhs(s[1], s[2], s[3], s[4], s[5], s[6], s[7], kp.a, kp.M));
+        if (kp.rcp_ok) {
+            bool ok;
+            const Rhs7 o = ks_rhs_rcp(s[1], s[2], s[3], s[4], s[5], s[6], s[7], kp.a, kp.M, ok);
+            if (ok) return to_v7(o);
+        }
+        return to_v7(ks_rhs_ieee(s[1], s[2], s[3], s[4], s[5], s[6], s[7], kp.a, kp.M));
     }
     static GRT_DEV void after_accept(double*, const KParams&, int) {}
 };
