@@ -147,12 +147,16 @@ class ClockSampler:
                 "source": f"NVML every {self.period * 1e3:.0f} ms during the timed regions"}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, collectives=True):
+    """(world, rank, local rank) from torchrun's environment; joins the NCCL
+    process group when several ranks run and `collectives` is set."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     import torch
-    if world > 1:
+    if world > 1 and not collectives:
+        torch.cuda.set_device(local)
+    elif world > 1:
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
@@ -550,7 +554,9 @@ def run_adjoint(args):
     import numpy as np
     import torch
     from grt import lib, workloads
-    dist_setup(args.gpus)
+    world, rank, _ = dist_setup(args.gpus, collectives=False)
+    if rank != 0:  # a one-GPU measurement: rank 0 runs it, the other ranks exit
+        return
     w = workloads.C4
     p = w.params()
     grid = w.torus()
@@ -595,7 +601,9 @@ def run_disk(args):
     scattering to escape or capture.  One step = emission + transport."""
     import torch
     from grt import lib, workloads
-    dist_setup(args.gpus)
+    world, rank, _ = dist_setup(args.gpus, collectives=False)
+    if rank != 0:  # a one-GPU measurement: rank 0 runs it, the other ranks exit
+        return
     w = workloads.C5
     p = w.params()
     stream = torch.cuda.Stream()

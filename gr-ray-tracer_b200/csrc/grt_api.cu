@@ -278,6 +278,10 @@ bool well_separated_increasing(const std::vector<double>& a) {
     return true;
 }
 
+// Shared memory a trace block may spend on staged separable axes (the RK45
+// stage slots take 35 KB of the 227 KB a block can have).
+constexpr size_t kMaxStagedAxisBytes = 160 * 1024;
+
 grt::KParams make_kparams(const grt_ctx* c) {
     const grt_params& p = c->p;
     grt::KParams k;
@@ -510,6 +514,10 @@ grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const 
             }
     sep = sep && well_separated_increasing(ra) && well_separated_increasing(ta) &&
           well_separated_increasing(pa) && ra[0] > 0.0 && pa[0] >= 0.0 && pa[nph - 1] < 2.0 * kPi;
+    // the staged axes and half-spans (16 bytes per axis value) must fit in
+    // shared memory beside the RK45 stage slots; longer axes use the general
+    // lookup on the full coordinate arrays
+    sep = sep && 16 * (nr + nth + nph) <= kMaxStagedAxisBytes;
     c->separable = sep;
     // Radii outside [lo, hi] fail within_radial_cell for every cell (margin
     // 0.6 > 0.500001 of the outermost log spacing), so lookup can stop early.

@@ -95,6 +95,19 @@ def test_nonseparable_grid_uses_general_lookup(gpu, oracle):
     assert_products_match(gprod, wprod)
 
 
+def test_long_separable_axes_use_general_lookup(gpu, oracle):
+    # nr + ntheta + nphi above the shared-memory budget for staged axes
+    # (10,240 values): the kernel keeps the axes in global memory and runs the
+    # general lookup, with the same results
+    w = mini(workloads.C2, 6, (10300, 2, 2))
+    p = w.params()
+    grid = w.torus()
+    got, gprod, _ = run_gpu(gpu, p, grid, nx=w.pixels, ny=w.pixels)
+    want, wprod, _ = run_oracle(oracle, p, grid, nx=w.pixels, ny=w.pixels)
+    assert_photons_match(got, want)
+    assert_products_match(gprod, wprod)
+
+
 def test_vacuum_grid(gpu, oracle):
     w = mini(workloads.C2, 8, (16, 8, 8))
     p = w.params()
