@@ -969,8 +969,9 @@ grt_status prepare_trace_buffers(grt_ctx* c, unsigned long long queue) {
 }
 
 // The trace of one chunk of the step loop: one launch over whole rays, or the
-// backward-leg launch and then, with the queue head reset, the forward-leg
-// launch over the same queue.
+// backward-leg launch, the packet generation of the rays it stopped at their
+// first fluid contact, and, with the queue head reset, the forward-leg launch
+// over the same queue.
 cudaError_t launch_trace(const grt_ctx* c, const grt::KParams& kp, size_t smem) {
     const grt_params& p = c->p;
     const bool mixed = p.precision == GRT_PREC_MIXED;
@@ -979,6 +980,10 @@ cudaError_t launch_trace(const grt_ctx* c, const grt::KParams& kp, size_t smem) 
     cudaError_t e = cudaMemsetAsync(kp.calls_carry, 0, kp.n * sizeof(long long), c->stream);
     if (e == cudaSuccess)
         e = grt::launch_trace(kp, mixed, 1, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+    if (e == cudaSuccess)
+        e = grt::launch_generate_pending(
+            kp, c->sm_count,
+            grt::dev_trace_smem_bytes(0, 128, c->fluid_available && c->separable, c->nr, c->nth, c->nph), c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(&kp.counters->queue_head, 0, sizeof(unsigned long long), c->stream);
     if (e == cudaSuccess)
         e = grt::launch_trace(kp, mixed, 2, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
@@ -1227,7 +1232,7 @@ grt_status run_steps(grt_ctx* c, grt_run_stats* stats, const OutputPlan* plan) {
         st.accepted_steps += k.accepted;
         st.rejected_attempts += k.rejected;
         st.photon_calls += k.calls;
-        st.launches += split_legs(c) ? 2 : 1;
+        st.launches += split_legs(c) ? 3 : 1;
         if (k.max_term_step > max_term_step) max_term_step = k.max_term_step;
         if (k.timed_out) {
             st.timed_out = 1;
@@ -1330,7 +1335,7 @@ grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
     st.accepted_steps = k.accepted;
     st.rejected_attempts = k.rejected;
     st.photon_calls = k.calls;
-    st.launches = split_legs(c) ? 2 : 1;
+    st.launches = split_legs(c) ? 3 : 1;
     st.n_terminated = k.terminated;
     st.trace_ms = ms;
     st.steps_done = single_launch_steps_done(p, k.terminated, c->n, k.max_term_step);

@@ -166,6 +166,10 @@ cudaError_t launch_trace_mixed_leg1(const KParams& kp, int integrator, int block
                                     cudaStream_t stream);
 cudaError_t launch_trace_mixed_leg2(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
                                     cudaStream_t stream);
+// Packet generation between the backward-leg and forward-leg launches
+// (photons with calls_carry < 0), one thread per queue index; smem holds the
+// staged axes (dev_trace_smem_bytes with integrator 0).
+cudaError_t launch_generate_pending(const KParams& kp, int sm_count, size_t smem, cudaStream_t stream);
 // sm_count * blocks_per_sm blocks of the form's (FP64 or mixed) kernel for `leg`.
 cudaError_t launch_trace(const KParams& kp, bool mixed, int leg, int integrator, int sm_count, int blocks_per_sm,
                          size_t smem, cudaStream_t stream);

@@ -96,15 +96,15 @@ struct Lane {
     int zero_all;         // a shared event zeroed every channel's Stokes vector
     long long pix;
     int fast;             // precision hint of the current call (mixed form)
-    int gen_pending;      // backward-leg launch: stopped at first fluid contact, generation left to leg 2
+    int gen_pending;      // backward-leg launch: stopped at first fluid contact, generation left to generate_body
     int need_k1;          // the call's k1 = f(state) is still to be evaluated
     double dl_try;
 };
 
 // GEO: the backward-leg launch, which neither reads nor changes a photon's
 // id, frequency, emission-frame energy, Stokes vector or screen position
-// (generation, transfer, scattering and arrival all happen in the forward-leg
-// launch): only the geodesic part is loaded and stored, and the Stokes vector
+// (generation happens in generate_body; transfer, scattering and arrival in
+// the forward-leg launch): only the geodesic part is loaded and stored, and the Stokes vector
 // only zeroed, which keeps those fields out of the lane's registers.
 template <bool GEO = false>
 GRT_DEV void load_photon(const KPhotons& P, long long i, Lane& L) {
@@ -176,8 +176,8 @@ GRT_DEV void store_follower(const KPhotons& P, const Lane& L, long long i, int t
 // Store the lane's photon and, in a sharing launch, every channel still riding
 // on its geodesic.  Returns the number of photons stored.  GEO (the
 // backward-leg launch, see load_photon): the geodesic part only, and no
-// followers when the ray is handed to the forward-leg launch with its
-// generation pending (that launch stores them).
+// followers when the ray is handed over with its generation pending (the
+// forward-leg launch stores them when the ray finishes).
 template <bool SHARE, bool GEO = false>
 GRT_DEV int store_all(const KParams& kp, const Lane& L, int terminated, double tdisp, double pdisp, int have_disp) {
     store_photon<GEO>(kp.ph, L, terminated, tdisp, pdisp, have_disp);
@@ -479,8 +479,8 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
     int terminated = 0;
     if (LEG != 2 && kp.image_mode && backward && sampled) {
         if (LEG == 1) {
-            // the backward-leg launch stops here: the forward-leg launch
-            // samples this position again and generates (one call, split)
+            // the backward-leg launch stops here: generate_body samples
+            // this position again and generates (one call, split)
             L.gen_pending = 1;
         } else {
             terminated = generate_at_contact<SHARE>(kp, L, fs, step, ch_term);
@@ -597,10 +597,9 @@ GRT_DEV void store_carry(const KParams& kp, const Lane& L) {
 //      photon over at its first fluid contact, before the packet generation
 //      of that call -- stored like a budget end, with the calls taken so far
 //      in KParams::calls_carry[q] (negated: -(calls + 1), generation pending);
-//   2  everything after: photons in any live phase but ImageBackward, and
-//      ImageBackward photons with a generation pending, which first finish
-//      that call (sample the same position again, generate); they resume
-//      with the calls the backward launch left in calls_carry[q].
+//      generate_body then finishes those calls, one thread per photon;
+//   2  everything after: photons in any live phase but ImageBackward,
+//      resuming with the calls left in calls_carry[q].
 // Each photon takes the same calls in the same order either way, so the two
 // launches give the one-launch result bit for bit; each loop body holds only
 // its own leg's code.
@@ -670,17 +669,12 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                         L.zero_all = 0;
                         slot = chan_slot(kp, lo, L.lead, L.pix);
                     }
-                    const long long carry = (LEG == 2 && q >= 0) ? kp.calls_carry[q] : 0;
                     if (q >= 0 && !kp.ph.terminate[slot] &&
-                        (LEG == 0 || (LEG == 1 && kp.ph.phase[slot] == 1) ||
-                         (LEG == 2 && (kp.ph.phase[slot] != 1 || carry < 0)))) {
+                        (LEG == 0 || ((kp.ph.phase[slot] == 1) == (LEG == 1)))) {
                         load_photon<LEG == 1>(kp.ph, slot, L);
                         L.idx = slot;
                         L.q = q;
-                        if (LEG == 2) {
-                            L.calls = carry < 0 ? -carry - 1 : carry;
-                            L.gen_pending = carry < 0 ? 1 : 0;
-                        }
+                        if (LEG == 2) L.calls = kp.calls_carry[q];
                         L.img = SHARE ? chan_image(kp, L.grp, L.lead) : image_of_photon(kp, q);
                         have_disp = 0;
                     }
@@ -700,24 +694,6 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
 
         // ---- one unit of work for this lane ----
         int finished = 0, terminated = 0;
-        if (LEG == 2 && L.gen_pending) {
-            // the rest of the call that reached the first fluid contact in
-            // the backward-leg launch: the same position samples the same
-            // cell, then the packet is generated
-            L.gen_pending = 0;
-            L.radius = ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
-            L.have_radius = 1;
-            FluidSample fs;
-            int ch_term = 0;
-            if (sample_fluid<RAW>(kp, ax, L.s, L.radius, fs))
-                terminated = generate_at_contact<SHARE>(kp, L, fs, kp.step0 + L.calls - 1, &ch_term);
-            if (SHARE && ch_term) {
-                cnt.terminated += ch_term;
-                const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
-                if (ts > cnt.max_term_step) cnt.max_term_step = ts;
-            }
-            finished = terminated;
-        } else {
         if (!L.mid_call) {
             if (L.calls >= kp.budget) {
                 finished = 1;  // budget of this launch used; photon stays live
@@ -793,7 +769,6 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                 }
             }
         }
-        }  // one call, or one RK45 attempt
         if (finished) {
             const int stored = store_all<SHARE, LEG == 1>(kp, L, terminated, tdisp, pdisp, have_disp);
             if (terminated) {
@@ -830,6 +805,78 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
         if (cnt.rejected) atomicAdd(&kp.counters->rejected, cnt.rejected);
         if (cnt.calls) atomicAdd(&kp.counters->calls, cnt.calls);
         if (cnt.max_term_step) atomicMax(&kp.counters->max_term_step, cnt.max_term_step);
+    }
+}
+
+// Between the backward-leg and forward-leg launches: the packet generation
+// of the rays the backward leg stopped at their first fluid contact
+// (calls_carry[q] < 0), one thread per queue index.  It finishes that call
+// (integrate_cart_ks.hpp:351-363): the same position samples the same cell,
+// the packet is generated, and the photon goes on to the forward-leg launch
+// in ImageForward with its calls in calls_carry[q] -- or terminates Rejected.
+// Kept out of the forward-leg loop, whose lanes would otherwise sit in this
+// once-per-ray code while their warp-mates step.
+template <bool SHARE>
+GRT_DEV void generate_body(const KParams& kp, const Axes& ax) {
+    unsigned long long terminated = 0, max_ts = 0;
+    const unsigned long long stride = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+    for (unsigned long long q = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; q < kp.n;
+         q += stride) {
+        const long long carry = kp.calls_carry[q];
+        if (carry >= 0) continue;
+        Lane L;
+        long long slot = static_cast<long long>(q);
+        if (SHARE) {
+            int lo = 0, hi = kp.ngroups - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (kp.group_qstart[mid] <= q) lo = mid;
+                else hi = mid - 1;
+            }
+            L.grp = lo;
+            L.pix = static_cast<long long>(q - kp.group_qstart[lo]);
+            L.nchan = kp.group_chan[lo + 1] - kp.group_chan[lo];
+            const unsigned long long ss = kp.share_state ? kp.share_state[q] : 0ull;
+            L.done = static_cast<unsigned>(ss & 0xFFFFFFFFull);
+            L.lead = static_cast<int>((ss >> 32) & 0xFFull);
+            slot = chan_slot(kp, lo, L.lead, L.pix);
+        }
+        load_photon<false>(kp.ph, slot, L);
+        L.idx = slot;
+        L.q = static_cast<long long>(q);
+        L.calls = -carry - 1;
+        L.img = SHARE ? chan_image(kp, L.grp, L.lead) : image_of_photon(kp, static_cast<long long>(q));
+        L.radius = ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
+        L.have_radius = 1;
+        FluidSample fs;
+        int ch_term = 0, term = 0;
+        if (sample_fluid<false>(kp, ax, L.s, L.radius, fs))
+            term = generate_at_contact<SHARE>(kp, L, fs, kp.step0 + L.calls - 1, &ch_term);
+        if (term || ch_term) {
+            const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
+            if (ts > max_ts) max_ts = ts;
+        }
+        terminated += static_cast<unsigned long long>(ch_term);
+        if (term) {
+            terminated += store_all<SHARE>(kp, L, 1, 0.0, 0.0, 0);
+        } else {
+            // the lead only: the followers' geodesic state is stored by the
+            // forward-leg launch when the ray finishes
+            store_photon(kp.ph, L, 0, 0.0, 0.0, 0);
+            kp.calls_carry[q] = L.calls;
+            if (SHARE && kp.share_state)
+                kp.share_state[q] = (static_cast<unsigned long long>(L.lead) << 32) | L.done;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        terminated += __shfl_down_sync(kFull, terminated, off);
+        const unsigned long long m = __shfl_down_sync(kFull, max_ts, off);
+        if (m > max_ts) max_ts = m;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (terminated) atomicAdd(&kp.counters->terminated, terminated);
+        if (max_ts) atomicMax(&kp.counters->max_term_step, max_ts);
     }
 }
 

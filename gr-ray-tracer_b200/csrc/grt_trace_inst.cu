@@ -70,4 +70,33 @@ cudaError_t GRT_LAUNCHER(const KParams& kp, int integrator, int blocks_per_sm, i
     }
 }
 
+#if GRT_LEG == 2 && !GRT_MIXED
+// Packet generation between the two legs (dev::generate_body): one thread per
+// queue index, the separable axes staged in shared memory for the lookup.
+template <bool SHARE>
+__global__ void __launch_bounds__(128) generate_pending(const __grid_constant__ KParams kp) {
+    extern __shared__ double smem[];
+    dev::Axes ax;
+    dev::KStore kk;
+    dev::stage_grid(kp, smem, 0, ax, kk);
+    dev::generate_body<SHARE>(kp, ax);
+}
+
+cudaError_t launch_generate_pending(const KParams& kp, int sm_count, size_t smem, cudaStream_t stream) {
+    if (kp.n == 0) return cudaSuccess;
+    const unsigned long long want = (kp.n + 127) / 128;
+    const unsigned long long cap = static_cast<unsigned long long>(sm_count) * 16;
+    const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
+    if (kp.ngroups > 0) {
+        cudaFuncSetAttribute(generate_pending<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        generate_pending<true><<<blocks, 128, smem, stream>>>(kp);
+    } else {
+        cudaFuncSetAttribute(generate_pending<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+        generate_pending<false><<<blocks, 128, smem, stream>>>(kp);
+    }
+    return cudaGetLastError();
+}
+#endif
+
 }  // namespace grt

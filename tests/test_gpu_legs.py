@@ -50,7 +50,7 @@ def assert_same(lib, p, grid, init, graph=False, sharing=True):
         assert int(x.arrived_count[0]) == int(y.arrived_count[0])
     for k in STATS:
         assert sa[k] == sb[k], (k, sa[k], sb[k])
-    assert sa["launches"] == 2 * sb["launches"]
+    assert sa["launches"] == 3 * sb["launches"]  # backward leg, generation, the rest
     assert sa["timed_out"] == 0
     return a, sa
 
@@ -93,7 +93,7 @@ def test_split_chunked_termination(gpu, sharing):
     p = w.params()
     specs = channel_batch(p)
     ph, st = assert_same(gpu, p, w.torus(), lambda c: c.init_image_batch(specs), sharing=sharing)
-    assert st["launches"] > 2 and st["steps_done"] < p.max_steps
+    assert st["launches"] > 3 and st["steps_done"] < p.max_steps
 
 
 def test_chunked_sharing_equals_unshared(gpu):
