@@ -372,8 +372,7 @@ def run_ours(args):
         ctx.upload_photons(host_in)
         ctx.run()
         if batched:
-            for k, out in enumerate(host_out):
-                ctx.batch_image_products(k, out)
+            ctx.all_batch_image_products(host_out)
         else:
             ctx.image_products(host_out[0])
 

@@ -1123,18 +1123,11 @@ grt_status grt_set_channel_sharing(grt_ctx* c, int enable) {
     return GRT_OK;
 }
 
-grt_status grt_get_batch_image_products(grt_ctx* c, size_t image, grt_image_products* out) {
-    if (!c || !out) return GRT_EINVAL;
-    if (!c->batched) return fail(c, GRT_ESTATE, "no image batch (grt_init_image_batch)");
-    if (image >= c->images.size()) return fail(c, GRT_EINVAL, "image index out of range");
+// Copies of image k's products into *out on the stream (the caller synchronises).
+static grt_status enqueue_batch_products(grt_ctx* c, size_t image, grt_image_products* out) {
     if (!out->image_I || !out->image_Q || !out->image_U || !out->image_V || !out->spectrum_frequency_hz ||
         !out->spectrum_I || !out->arrived_count)
         return fail(c, GRT_EINVAL, "null image product buffer");
-    if (!c->bproducts_valid) {
-        grt_status st = launch_all_products(c);
-        if (st != GRT_OK) return st;
-        c->bproducts_valid = true;
-    }
     const grt_image_spec& sp = c->images[image];
     const size_t npix = sp.nx * sp.ny, bins = c->p.spectrum_bins;
     const double* src = c->bimage.ptr + c->bimage_off[image];
@@ -1147,6 +1140,39 @@ grt_status grt_get_batch_image_products(grt_ctx* c, size_t image, grt_image_prod
     GRT_CUDA(c, cudaMemcpyAsync(out->arrived_count, c->barrived.ptr + image, sizeof(unsigned long long),
                                 cudaMemcpyDeviceToHost, c->stream), "D2H arrived");
     fill_spectrum_frequencies(c->p, out->spectrum_frequency_hz);
+    return GRT_OK;
+}
+
+static grt_status ensure_batch_products(grt_ctx* c) {
+    if (!c->batched) return fail(c, GRT_ESTATE, "no image batch (grt_init_image_batch)");
+    if (!c->bproducts_valid) {
+        grt_status st = launch_all_products(c);
+        if (st != GRT_OK) return st;
+        c->bproducts_valid = true;
+    }
+    return GRT_OK;
+}
+
+grt_status grt_get_batch_image_products(grt_ctx* c, size_t image, grt_image_products* out) {
+    if (!c || !out) return GRT_EINVAL;
+    grt_status st = ensure_batch_products(c);
+    if (st != GRT_OK) return st;
+    if (image >= c->images.size()) return fail(c, GRT_EINVAL, "image index out of range");
+    st = enqueue_batch_products(c, image, out);
+    if (st != GRT_OK) return st;
+    GRT_CUDA(c, cudaStreamSynchronize(c->stream), "products");
+    return GRT_OK;
+}
+
+grt_status grt_get_all_batch_image_products(grt_ctx* c, grt_image_products* outs, size_t nimages) {
+    if (!c || (!outs && nimages)) return GRT_EINVAL;
+    grt_status st = ensure_batch_products(c);
+    if (st != GRT_OK) return st;
+    if (nimages != c->images.size()) return fail(c, GRT_EINVAL, "nimages must equal the batch's image count");
+    for (size_t k = 0; k < nimages; ++k) {
+        st = enqueue_batch_products(c, k, outs + k);
+        if (st != GRT_OK) return st;
+    }
     GRT_CUDA(c, cudaStreamSynchronize(c->stream), "products");
     return GRT_OK;
 }

@@ -99,6 +99,8 @@ def load(path: Path | None = None):
                                                C.c_size_t]
     L.grt_write_output_step_npz.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int64, C.c_int32, C.c_char_p, C.c_uint64]
     L.grt_run_with_output.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64, P(RunStats)]
+    L.grt_get_all_batch_image_products.argtypes = [vp, P(ImageProducts), C.c_size_t]
+    L.grt_get_all_batch_image_products.restype = C.c_int
     L.grt_photon_block_bytes.argtypes = [C.c_size_t]
     L.grt_photon_block_bytes.restype = C.c_size_t
     L.grt_host_photon_layout.argtypes = [vp, C.c_size_t, P(PhotonSoA)]
@@ -298,6 +300,12 @@ class Context:
         s = out.struct()
         self._check(self.lib.grt_get_batch_image_products(self._h, image, C.byref(s)))
         return out
+
+    def all_batch_image_products(self, outs: list) -> list:
+        """Every image's products (outs[k]: ProductArrays for image k) with one synchronisation."""
+        arr = (ImageProducts * len(outs))(*[o.struct() for o in outs])
+        self._check(self.lib.grt_get_all_batch_image_products(self._h, arr, len(outs)))
+        return outs
 
     def write_batch_products_npz(self, output_dir, name):
         self._check(self.lib.grt_write_batch_products_npz(self._h, str(output_dir).encode(), name.encode()))

@@ -395,6 +395,9 @@ grt_status grt_set_channel_sharing(grt_ctx* ctx, int enable);
 
 /* Products of image k of the batch (buffers sized nx_k*ny_k and p.spectrum_bins). */
 grt_status grt_get_batch_image_products(grt_ctx* ctx, size_t image, grt_image_products* out);
+/* Every image's products of the batch at once, outs[k] for image k (nimages
+ * = grt_batch_image_count): the copies of all images and one synchronisation. */
+grt_status grt_get_all_batch_image_products(grt_ctx* ctx, grt_image_products* outs, size_t nimages);
 
 /* Write <output_dir>/<name>_image<k>_image_products.npz for every image k. */
 grt_status grt_write_batch_products_npz(grt_ctx* ctx, const char* output_dir, const char* name);

@@ -221,3 +221,24 @@ def test_channel_sharing_equals_single_images(gpu, oracle, generator):
         assert_products_match(sprods[k], wprod)
         start += n
     assert n_shared_geodesics < shared.n
+
+
+def test_all_batch_products_at_once(gpu):
+    # grt_get_all_batch_image_products: the same products as one call per image
+    p = SMALL.params()
+    specs = batch_specs(p)
+    ctx = gpu.Context(p)
+    try:
+        ctx.upload_grid(SMALL.torus())
+        ctx.init_image_batch(specs)
+        ctx.run()
+        each = [ctx.batch_image_products(k) for k in range(len(specs))]
+        outs = [abi.ProductArrays(sp.nx, sp.ny, p.spectrum_bins) for sp in specs]
+        ctx.all_batch_image_products(outs)
+        with pytest.raises(Exception, match="nimages"):
+            ctx.all_batch_image_products(outs[:1])
+    finally:
+        ctx.close()
+    for a, b in zip(outs, each):
+        for f in ("image_I", "image_Q", "image_U", "image_V", "spectrum_frequency_hz", "spectrum_I", "arrived_count"):
+            assert np.array_equal(getattr(a, f), getattr(b, f)), f
