@@ -52,10 +52,11 @@ __global__ void init_image_pixels(const __grid_constant__ InitImageArgs args) {
 
 
 // observation.hpp:61-82: ImageArrived photons binned by arrival (u, v) and
-// log10(nu).  Each block serves one image of the set; its spectrum is summed
-// in shared memory first (the arrival frequencies of an image crowd into a few
-// bins, so per-photon global atomics would serialise on them) and flushed with
-// one global atomic per non-empty bin.
+// log10(nu).  Each block serves one image of the set.  The arrival
+// frequencies of an image crowd into a few spectrum bins, so per-photon
+// atomics would serialise on them: the spectrum is summed per warp (one
+// shuffle reduction per distinct bin), then per block in shared memory, and
+// flushed with one global atomic per non-empty bin.
 __global__ void __launch_bounds__(256) image_products(const __grid_constant__ ProductsSet set) {
     extern __shared__ double hist[];
     __shared__ unsigned long long s_arrived;
@@ -70,24 +71,44 @@ __global__ void __launch_bounds__(256) image_products(const __grid_constant__ Pr
     if (threadIdx.x == 0) s_arrived = 0;
     __syncthreads();
     const unsigned long long npix = im.nx * im.ny;
+    const unsigned lane = threadIdx.x & 31u;
     unsigned long long count = 0;
-    for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x - im.block0) * blockDim.x + threadIdx.x;
-         i < im.n; i += stride) {
+    // warp-uniform trip count: every lane of a warp runs each iteration, so
+    // the spectrum can be summed per warp before the shared-memory atomics
+    for (unsigned long long i0 = static_cast<unsigned long long>(blockIdx.x - im.block0) * blockDim.x +
+                                 (threadIdx.x & ~31u);
+         i0 < im.n; i0 += stride) {
+        const unsigned long long i = i0 + lane;
         const unsigned long long o = im.offset + i;
-        if (set.ph.phase[o] != 3) continue;
-        ++count;
-        const unsigned long long px = dev::observation_bin(set.ph.theta_disp[o], -0.5 * im.W, 0.5 * im.W, im.nx);
-        const unsigned long long py = dev::observation_bin(set.ph.phi_disp[o], -0.5 * im.H, 0.5 * im.H, im.ny);
-        const unsigned long long pix = py * im.nx + px;
-        const double I = set.ph.I[o];
-        atomicAdd(&im.image[pix], I);
-        atomicAdd(&im.image[npix + pix], set.ph.Q[o]);
-        atomicAdd(&im.image[2 * npix + pix], set.ph.U[o]);
-        atomicAdd(&im.image[3 * npix + pix], set.ph.V[o]);
-        const double f = set.ph.frequency[o];
-        if (set.bins > 0 && f >= set.spec_min && f <= set.spec_max) {
-            const unsigned long long b = dev::observation_bin(log10(f), set.log_min, set.log_max, set.bins);
-            atomicAdd(shared_spec ? &hist[b] : &im.spectrum[b], I);
+        long long b = -1;
+        double I = 0.0;
+        if (i < im.n && set.ph.phase[o] == 3) {
+            ++count;
+            const unsigned long long px =
+                dev::observation_bin(set.ph.theta_disp[o], -0.5 * im.W, 0.5 * im.W, im.nx);
+            const unsigned long long py =
+                dev::observation_bin(set.ph.phi_disp[o], -0.5 * im.H, 0.5 * im.H, im.ny);
+            const unsigned long long pix = py * im.nx + px;
+            I = set.ph.I[o];
+            atomicAdd(&im.image[pix], I);
+            atomicAdd(&im.image[npix + pix], set.ph.Q[o]);
+            atomicAdd(&im.image[2 * npix + pix], set.ph.U[o]);
+            atomicAdd(&im.image[3 * npix + pix], set.ph.V[o]);
+            const double f = set.ph.frequency[o];
+            if (set.bins > 0 && f >= set.spec_min && f <= set.spec_max)
+                b = static_cast<long long>(dev::observation_bin(log10(f), set.log_min, set.log_max, set.bins));
+        }
+        // one sum per distinct bin of the warp (few: an image's arrival
+        // frequencies crowd into a handful of bins), then one atomic
+        unsigned pending = __ballot_sync(0xFFFFFFFFu, b >= 0);
+        while (pending) {
+            const long long b0 = __shfl_sync(0xFFFFFFFFu, b, __ffs(pending) - 1);
+            const unsigned members = __ballot_sync(0xFFFFFFFFu, b == b0);
+            double v = b == b0 ? I : 0.0;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, off);
+            if (lane == 0) atomicAdd(shared_spec ? &hist[b0] : &im.spectrum[b0], v);
+            pending &= ~members;
         }
     }
 #pragma unroll
