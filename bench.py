@@ -463,13 +463,14 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def cpu_baseline(w, reps=2):
+def cpu_baseline(w, reps=2, params=None, label=None):
     """The reference's own integrate_geodesics (shim-compiled, oracle/_ref) on
-    the host cores, on the full workload; falls back to the oracle port."""
+    the host cores, on one full image of workload w (params: that image's
+    parameters, default w's); falls back to the oracle port."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
     from grt import config, torus
-    p = w.params()
+    p = params if params is not None else w.params()
     n = w.pixels * w.pixels
     with tempfile.TemporaryDirectory() as d:
         d = Path(d)
@@ -498,24 +499,45 @@ def cpu_baseline(w, reps=2):
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     return {"value": n / best[0], "unit": "rays/s", "rk_steps_per_s": best[1] / best[0], "cores": cores,
             "kind": kind,
-            "sample": f"full {w.name} workload ({n} rays), best of {reps}; reference Kokkos functor via the "
-                      "project OpenMP shim (real Kokkos is not installable offline), OMP threads = all cores"}
+            "sample": f"{label or 'full ' + w.name + ' workload'} ({n} rays), best of {reps}; reference Kokkos "
+                      "functor via the project OpenMP shim (real Kokkos is not installable offline), "
+                      "OMP threads = all cores"}
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU code (oracle/_ref) on the
+    workload of our arm -- for the default, the C2 image at its four frequency
+    channels.  The reference traces one camera per run, so each step is one
+    channel's full 256x256 image (a bounded sample of the batch), cycling
+    through the channels; rays/s is the batch's metric."""
+    import math
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from grt import workloads
     w = workloads.WORKLOADS[args.workload]
+    bw = workloads.BATCHES.get(args.workload)
+    # one parameter set per channel image of the batch with w's resolution
+    chans = []
+    if bw is not None:
+        for incl, px, f_ghz in bw.images:
+            if px != w.pixels:
+                continue
+            q = w.params()
+            q.update(camera_theta=math.radians(incl), custom_frequency_hz=f_ghz * 1e9,
+                     emission_coefficient=q.emission_coefficient * f_ghz / 230.0)
+            chans.append((q, f"{incl:g} deg, {f_ghz:g} GHz"))
+    if not chans:
+        chans = [(w.params(), w.name)]
     vals = []
-    for _ in range(args.warmup):
-        cpu_baseline(w, reps=1)
+    for i in range(args.warmup):
+        cpu_baseline(w, reps=1, params=chans[i % len(chans)][0])
     t_total = 0.0
     steps_total = 0.0
-    for _ in range(args.steps):
-        c = cpu_baseline(w, reps=1)
+    for i in range(args.steps):
+        q, lab = chans[i % len(chans)]
+        c = cpu_baseline(w, reps=1, params=q, label=f"one {w.pixels}x{w.pixels} channel image per step ({lab})")
         vals.append(c)
         t_total += (w.pixels * w.pixels) / c["value"]
         steps_total += c["rk_steps_per_s"] * (w.pixels * w.pixels) / c["value"]
@@ -527,7 +549,9 @@ def run_reference(args):
         "rk_steps_per_s": steps_total / t_total, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w.name, "pixels": f"{w.pixels}x{w.pixels}", "grid": "x".join(map(str, w.grid))},
+        "config": {"workload": bw.name if bw is not None else w.name, "pixels": f"{w.pixels}x{w.pixels}",
+                   "grid": "x".join(map(str, w.grid)),
+                   "sample": f"one channel image per step, cycling through {len(chans)} channel(s)"},
         "cpu_baseline": {"value": value, "unit": "rays/s", "cores": c["cores"], "kind": c["kind"],
                          "sample": c["sample"]},
         "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
