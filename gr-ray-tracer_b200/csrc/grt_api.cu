@@ -957,8 +957,9 @@ unsigned long long iteration_limit(const grt::KParams& kp, unsigned long long to
            (1ull << 20);
 }
 
-// Image-mode rays are traced by two launches, the backward leg then the rest
-// (trace_body LEG 1 and 2), unless the launch shape asks for one.
+// Image-mode rays are traced by the backward-leg launch, the packet generation
+// at first fluid contact and the launch over the rest (trace_body LEG 1 and
+// 2), unless the launch shape asks for one launch over whole rays.
 bool split_legs(const grt_ctx* c) { return c->lc.split_legs != 0 && c->p.mode == GRT_MODE_IMAGE; }
 
 // Device buffers a trace needs besides the photons; allocated before any

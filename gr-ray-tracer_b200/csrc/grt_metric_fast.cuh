@@ -1,5 +1,5 @@
 // FP32 right-hand side of Hamilton's equations for the mixed trace form
-// (grt_kernels_mixed.cu).  Same mathematics as ks_rhs (grt_metric.cuh;
+// (MixedRhs in grt_rhs_mixed.cuh).  Same mathematics as ks_rhs (grt_metric.cuh;
 // reference kerr_schild_core.hpp:157-192), reorganised for FP32 throughput:
 // the 21 divisions and 2 square roots become 2 reciprocal square roots and 2
 // reciprocals on the special-function unit, and the multiply-adds are

@@ -591,7 +591,8 @@ GRT_DEV void store_carry(const KParams& kp, const Lane& L) {
 }
 
 // SHARE: queue indices are geodesics of channel groups (KParams::ngroups > 0).
-// LEG splits an image-mode launch into two launches over the same queue:
+// LEG splits an image-mode launch into two trace launches over the same queue,
+// with the generate_pending kernel between them:
 //   0  whole rays (disk mode, or image mode in one launch);
 //   1  the backward leg: photons in ImageBackward only; a lane hands its
 //      photon over at its first fluid contact, before the packet generation
@@ -600,7 +601,7 @@ GRT_DEV void store_carry(const KParams& kp, const Lane& L) {
 //      generate_body then finishes those calls, one thread per photon;
 //   2  everything after: photons in any live phase but ImageBackward,
 //      resuming with the calls left in calls_carry[q].
-// Each photon takes the same calls in the same order either way, so the two
+// Each photon takes the same calls in the same order either way, so the split
 // launches give the one-launch result bit for bit; each loop body holds only
 // its own leg's code.
 template <int INTEGRATOR, class RHS, bool RAW = false, bool SHARE = false, int LEG = 0>

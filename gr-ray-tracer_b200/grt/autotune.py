@@ -3,8 +3,8 @@
 Searches the occupancy class (resident 128-thread blocks per SM, i.e. the
 register cap of the kernel instantiation), the per-warp refill threshold (idle
 lanes before a warp pulls new photons), the photons a warp claims per queue
-access and, in image mode, whether the rays' backward and forward legs run as
-two launches or one, timing each candidate with the library's own CUDA
+access and, in image mode, whether the rays' backward leg and the rest run as
+split launches (backward leg, packet generation, the rest) or one, timing each candidate with the library's own CUDA
 events around the trace launch on the actual workload.  Results are cached per
 (workload key, precision, integrator) for the life of the process.
 """
@@ -18,7 +18,7 @@ _CACHE: dict = {}
 BLOCKS_PER_SM = (2, 3, 4)   # 128-thread blocks; register caps 255 / 170 / 128
 REFILL = (1, 8, 16, 32)
 GRAB = (32, 128)
-SPLIT_LEGS = (1, 0)         # image mode: backward leg and the rest as two launches, or one
+SPLIT_LEGS = (1, 0)         # image mode: split legs (three launches per chunk), or one launch
 
 
 def candidates(image_mode: bool = True):
