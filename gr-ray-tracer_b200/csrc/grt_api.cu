@@ -198,6 +198,12 @@ struct grt_ctx {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     uint64_t generation = 1, graph_generation = 0;
+    // asynchronous renders (grt_render_async / grt_render_wait): the photon
+    // upload and the products' copy-back run on copy_stream, the trace on
+    // stream; one render in flight per context
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_uploaded = nullptr, ev_traced = nullptr, ev_done = nullptr;
+    bool render_pending = false;
 };
 
 namespace {
@@ -400,7 +406,11 @@ grt_status grt_create(const grt_params* p, grt_ctx** out) {
         c->counters.alloc(1) != cudaSuccess || c->scratch_u64.alloc(4) != cudaSuccess ||
         cudaMallocHost(reinterpret_cast<void**>(&c->host_counters), sizeof(grt::KCounters)) != cudaSuccess ||
         cudaMallocHost(reinterpret_cast<void**>(&c->host_u64), 4 * sizeof(unsigned long long)) != cudaSuccess ||
-        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_uploaded, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_traced, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming) != cudaSuccess) {
         grt_destroy(c);
         return GRT_ECUDA;
     }
@@ -412,6 +422,7 @@ grt_status grt_create(const grt_params* p, grt_ctx** out) {
 void grt_destroy(grt_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     c->r_axis.release(); c->th_axis.release(); c->ph_axis.release();
     c->r_half.release(); c->th_half.release(); c->ph_half.release();
     c->r3.release(); c->th3.release(); c->ph3.release();
@@ -434,6 +445,10 @@ void grt_destroy(grt_ctx* c) {
     if (c->host_u64) cudaFreeHost(c->host_u64);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->ev_uploaded) cudaEventDestroy(c->ev_uploaded);
+    if (c->ev_traced) cudaEventDestroy(c->ev_traced);
+    if (c->ev_done) cudaEventDestroy(c->ev_done);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -1124,22 +1139,25 @@ grt_status grt_set_channel_sharing(grt_ctx* c, int enable) {
     return GRT_OK;
 }
 
-// Copies of image k's products into *out on the stream (the caller synchronises).
-static grt_status enqueue_batch_products(grt_ctx* c, size_t image, grt_image_products* out) {
-    if (!out->image_I || !out->image_Q || !out->image_U || !out->image_V || !out->spectrum_frequency_hz ||
-        !out->spectrum_I || !out->arrived_count)
-        return fail(c, GRT_EINVAL, "null image product buffer");
+static bool products_complete(const grt_image_products* out) {
+    return out->image_I && out->image_Q && out->image_U && out->image_V && out->spectrum_frequency_hz &&
+           out->spectrum_I && out->arrived_count;
+}
+
+// Copies of image k's products into *out on stream st (the caller synchronises).
+static grt_status enqueue_batch_products(grt_ctx* c, size_t image, grt_image_products* out, cudaStream_t st) {
+    if (!products_complete(out)) return fail(c, GRT_EINVAL, "null image product buffer");
     const grt_image_spec& sp = c->images[image];
     const size_t npix = sp.nx * sp.ny, bins = c->p.spectrum_bins;
     const double* src = c->bimage.ptr + c->bimage_off[image];
     double* dst[4] = {out->image_I, out->image_Q, out->image_U, out->image_V};
     for (int q = 0; q < 4; ++q)
-        GRT_CUDA(c, cudaMemcpyAsync(dst[q], src + q * npix, npix * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+        GRT_CUDA(c, cudaMemcpyAsync(dst[q], src + q * npix, npix * sizeof(double), cudaMemcpyDeviceToHost, st),
                  "D2H image");
     GRT_CUDA(c, cudaMemcpyAsync(out->spectrum_I, c->bspectrum.ptr + image * bins, bins * sizeof(double),
-                                cudaMemcpyDeviceToHost, c->stream), "D2H spectrum");
+                                cudaMemcpyDeviceToHost, st), "D2H spectrum");
     GRT_CUDA(c, cudaMemcpyAsync(out->arrived_count, c->barrived.ptr + image, sizeof(unsigned long long),
-                                cudaMemcpyDeviceToHost, c->stream), "D2H arrived");
+                                cudaMemcpyDeviceToHost, st), "D2H arrived");
     fill_spectrum_frequencies(c->p, out->spectrum_frequency_hz);
     return GRT_OK;
 }
@@ -1159,7 +1177,7 @@ grt_status grt_get_batch_image_products(grt_ctx* c, size_t image, grt_image_prod
     grt_status st = ensure_batch_products(c);
     if (st != GRT_OK) return st;
     if (image >= c->images.size()) return fail(c, GRT_EINVAL, "image index out of range");
-    st = enqueue_batch_products(c, image, out);
+    st = enqueue_batch_products(c, image, out, c->stream);
     if (st != GRT_OK) return st;
     GRT_CUDA(c, cudaStreamSynchronize(c->stream), "products");
     return GRT_OK;
@@ -1171,7 +1189,7 @@ grt_status grt_get_all_batch_image_products(grt_ctx* c, grt_image_products* outs
     if (st != GRT_OK) return st;
     if (nimages != c->images.size()) return fail(c, GRT_EINVAL, "nimages must equal the batch's image count");
     for (size_t k = 0; k < nimages; ++k) {
-        st = enqueue_batch_products(c, k, outs + k);
+        st = enqueue_batch_products(c, k, outs + k, c->stream);
         if (st != GRT_OK) return st;
     }
     GRT_CUDA(c, cudaStreamSynchronize(c->stream), "products");
@@ -1366,6 +1384,118 @@ grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
     st.n_terminated = k.terminated;
     st.trace_ms = ms;
     st.steps_done = single_launch_steps_done(p, k.terminated, c->n, k.max_term_step);
+    if (k.timed_out) {
+        st.timed_out = 1;
+        if (stats) *stats = st;
+        return fail(c, GRT_ETIMEOUT, "trace kernel hit its iteration limit");
+    }
+    if (stats) *stats = st;
+    return GRT_OK;
+}
+
+// Enqueue one render of uploaded photons: the host photon block goes up on
+// copy_stream; the trace launches and every image's products follow on stream
+// once it has landed; the products go back on copy_stream once they are
+// built.  Nothing synchronises here.
+static grt_status enqueue_render(grt_ctx* c, const grt_photon_soa* s, grt_image_products* outs) {
+    const size_t n = c->n, nimg = c->images.size();
+    grt::KParams kp = make_kparams(c);
+    kp.calls_carry = c->calls_carry.ptr;
+    kp.step0 = 0;
+    kp.budget = c->p.max_steps;
+    kp.max_iterations = iteration_limit(kp, n, c->sm_count * c->lc.blocks_per_sm, 128);
+    GRT_CUDA(c, cudaMemcpyAsync(c->ph.block.ptr, s->id, grt_photon_block_bytes(n), cudaMemcpyHostToDevice,
+                                c->copy_stream), "H2D photons");
+    GRT_CUDA(c, cudaEventRecord(c->ev_uploaded, c->copy_stream), "event");
+    GRT_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_uploaded, 0), "stream wait");
+    if (c->groups_share && c->geodesics)
+        GRT_CUDA(c, cudaMemsetAsync(c->share_state.ptr, 0, c->geodesics * sizeof(unsigned long long), c->stream),
+                 "memset share state");
+    // photons terminated before the trace count toward the stop rule
+    GRT_CUDA(c, cudaMemsetAsync(c->scratch_u64.ptr + 1, 0, sizeof(unsigned long long), c->stream), "memset");
+    GRT_CUDA(c, grt::launch_count_terminated(c->ph.term.ptr, n, c->scratch_u64.ptr + 1, c->sm_count, c->stream),
+             "count_terminated");
+    GRT_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, sizeof(grt::KCounters), c->stream), "memset counters");
+    GRT_CUDA(c, cudaEventRecord(c->ev0, c->stream), "event");
+    const cudaError_t e = launch_trace(c, kp, trace_smem(c));
+    if (e != cudaSuccess) return cuda_fail(c, e, "trace launch");
+    GRT_CUDA(c, cudaEventRecord(c->ev1, c->stream), "event");
+    grt_status st = launch_all_products(c);
+    if (st != GRT_OK) return st;
+    GRT_CUDA(c, cudaMemcpyAsync(c->host_counters, c->counters.ptr, sizeof(grt::KCounters), cudaMemcpyDeviceToHost,
+                                c->stream), "D2H counters");
+    GRT_CUDA(c, cudaMemcpyAsync(c->host_u64 + 1, c->scratch_u64.ptr + 1, sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, c->stream), "D2H count");
+    GRT_CUDA(c, cudaEventRecord(c->ev_traced, c->stream), "event");
+    GRT_CUDA(c, cudaStreamWaitEvent(c->copy_stream, c->ev_traced, 0), "stream wait");
+    for (size_t k = 0; k < nimg; ++k) {
+        st = enqueue_batch_products(c, k, outs + k, c->copy_stream);
+        if (st != GRT_OK) return st;
+    }
+    GRT_CUDA(c, cudaEventRecord(c->ev_done, c->copy_stream), "event");
+    return GRT_OK;
+}
+
+grt_status grt_render_async(grt_ctx* c, const grt_photon_soa* s, grt_image_products* outs, size_t nimages) {
+    if (!c || !s || (!outs && nimages)) return GRT_EINVAL;
+    if (c->render_pending) return fail(c, GRT_ESTATE, "a render is in flight on this context (grt_render_wait)");
+    if (!c->grid_uploaded) return fail(c, GRT_ESTATE, "grt_render_async before grt_upload_grid");
+    if (!c->batched || !c->have_images || c->n == 0)
+        return fail(c, GRT_ESTATE, "grt_render_async needs an image batch (grt_init_image_batch)");
+    const grt_params& p = c->p;
+    if (!(p.termination_percent >= 1.0))
+        return fail(c, GRT_EINVAL, "grt_render_async needs termination_percent >= 1 (one trace launch)");
+    if (nimages != c->images.size()) return fail(c, GRT_EINVAL, "nimages must equal the batch's image count");
+    if (!soa_is_block(s, c->n))
+        return fail(c, GRT_EINVAL,
+                    "grt_render_async takes the batch's photons as one host block (grt_host_photon_layout, "
+                    "grt_photon_count photons)");
+    for (size_t k = 0; k < nimages; ++k)
+        if (!products_complete(outs + k)) return fail(c, GRT_EINVAL, "null image product buffer");
+    // allocations before anything is enqueued
+    {
+        const grt_status bs = prepare_trace_buffers(c, make_kparams(c).n);
+        if (bs != GRT_OK) return bs;
+        size_t pix = 0;
+        for (const auto& sp : c->images) pix += 4 * sp.nx * sp.ny;
+        GRT_CUDA(c, c->bimage.alloc(pix), "alloc products");
+        GRT_CUDA(c, c->bspectrum.alloc(nimages * p.spectrum_bins), "alloc products");
+        GRT_CUDA(c, c->barrived.alloc(nimages), "alloc products");
+    }
+    c->bproducts_valid = false;
+    c->adj_ready = false;
+    const grt_status st = enqueue_render(c, s, outs);
+    if (st != GRT_OK) {
+        // part of the render may be enqueued: let it drain before reporting
+        cudaStreamSynchronize(c->stream);
+        cudaStreamSynchronize(c->copy_stream);
+        return st;
+    }
+    c->render_pending = true;
+    return GRT_OK;
+}
+
+grt_status grt_render_wait(grt_ctx* c, grt_run_stats* stats) {
+    if (!c) return GRT_EINVAL;
+    if (!c->render_pending) return fail(c, GRT_ESTATE, "no render in flight on this context (grt_render_async)");
+    c->render_pending = false;
+    GRT_CUDA(c, cudaEventSynchronize(c->ev_done), "render");
+    const grt_params& p = c->p;
+    const grt::KCounters& k = *c->host_counters;
+    const unsigned long long terminated = c->host_u64[1] + k.terminated;
+    c->initial_terminated = terminated;
+    c->bproducts_valid = true;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    grt_run_stats st;
+    std::memset(&st, 0, sizeof(st));
+    st.accepted_steps = k.accepted;
+    st.rejected_attempts = k.rejected;
+    st.photon_calls = k.calls;
+    st.launches = split_legs(c) ? 3 : 1;
+    st.n_terminated = terminated;
+    st.trace_ms = ms;
+    st.steps_done = single_launch_steps_done(p, terminated, c->n, k.max_term_step);
     if (k.timed_out) {
         st.timed_out = 1;
         if (stats) *stats = st;

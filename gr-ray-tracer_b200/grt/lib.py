@@ -105,6 +105,10 @@ def load(path: Path | None = None):
     L.grt_photon_block_bytes.restype = C.c_size_t
     L.grt_host_photon_layout.argtypes = [vp, C.c_size_t, P(PhotonSoA)]
     L.grt_host_photon_layout.restype = C.c_int
+    L.grt_render_async.argtypes = [vp, P(PhotonSoA), P(ImageProducts), C.c_size_t]
+    L.grt_render_async.restype = C.c_int
+    L.grt_render_wait.argtypes = [vp, P(RunStats)]
+    L.grt_render_wait.restype = C.c_int
     for name in ("grt_parse_output_variables", "grt_output_options_from_toml", "grt_write_output_step_npz",
                  "grt_run_with_output", "grt_set_cell_multipliers", "grt_forward_checkpointed", "grt_adjoint_image_I",
                  "grt_init_image_batch", "grt_get_batch_image_products", "grt_write_batch_products_npz",
@@ -314,6 +318,23 @@ class Context:
         """Re-initialise, trace and build products through the context's CUDA graph."""
         st = RunStats()
         rc = self.lib.grt_render_graph(self._h, C.byref(st))
+        self._check(rc)
+        return st.as_dict()
+
+    def render_async(self, photons: PhotonArrays, outs: list):
+        """Enqueue a render of host photons (a PhotonArrays.block of the batch's
+        count, pinned for overlap) into outs (ProductArrays per image); returns
+        at once.  photons and outs stay in use until render_wait."""
+        soa = photons.soa()
+        arr = (ImageProducts * len(outs))(*[o.struct() for o in outs])
+        self._check(self.lib.grt_render_async(self._h, C.byref(soa), arr, len(outs)))
+        self._pending = (photons, outs, soa, arr)
+
+    def render_wait(self) -> dict:
+        """Wait for the render in flight; its products are then in its outs."""
+        st = RunStats()
+        rc = self.lib.grt_render_wait(self._h, C.byref(st))
+        self._pending = None
         self._check(rc)
         return st.as_dict()
 

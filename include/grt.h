@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define GRT_ABI_VERSION 3
+#define GRT_ABI_VERSION 4
 
 typedef enum grt_status {
     GRT_OK = 0,
@@ -414,6 +414,26 @@ grt_status grt_write_batch_products_npz(grt_ctx* ctx, const char* output_dir, co
  * grt_get_batch_image_products.
  */
 grt_status grt_render_graph(grt_ctx* ctx, grt_run_stats* stats);
+
+/*
+ * Asynchronous render of host photons (no counterpart in the reference, whose
+ * step loop is synchronous; integrate_cart_ks.hpp:468-527 with the products
+ * of observation.hpp:31-84).  grt_render_async enqueues, without waiting:
+ * the copy of `photons` (a host photon block of grt_photon_count photons,
+ * grt_host_photon_layout; pinned for the copy to overlap) into the batch's
+ * slots on the context's copy stream; the trace and every image's products on
+ * the context's stream once the copy has landed; and the copy of the products
+ * into outs[k] (as grt_get_all_batch_image_products) on the copy stream.
+ * The batch keeps its images, as grt_upload_photons with the batch's count
+ * does.  Needs an image batch and termination_percent >= 1.  The host buffers
+ * must stay untouched until grt_render_wait returns; one render is in flight
+ * per context (GRT_ESTATE otherwise).  Two contexts given the same stream
+ * (grt_set_stream) and used in turn keep their traces in order on it while
+ * one's copies overlap the other's trace.  grt_render_wait blocks until the
+ * render's products are on the host and fills stats as grt_run does.
+ */
+grt_status grt_render_async(grt_ctx* ctx, const grt_photon_soa* photons, grt_image_products* outs, size_t nimages);
+grt_status grt_render_wait(grt_ctx* ctx, grt_run_stats* stats);
 
 /*
  * Differentiable radiative transfer (no counterpart in the reference).

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_function():
     assert len(names) >= 20
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
-    assert L.grt_abi_version() == 3
+    assert L.grt_abi_version() == 4
 
 
 def test_struct_layout_matches_c(tmp_path):
