@@ -699,15 +699,18 @@ def run_disk(args):
     ctx = lib.Context(p)
     ctx.set_stream(stream.cuda_stream)
     ctx.upload_grid(w.torus())
+    n = ctx.init_disk_photons()
+    q = p.copy()
+    q.nphotons = n
+    ctx.set_params(q)
+    if not args.no_autotune:
+        from grt import autotune
+        autotune.tune(ctx, lambda c: c.init_disk_photons(), w.name, reps=1)
+    cfg = ctx.launch_config()
     init_ms = run_ms = 0.0
     st = None
-    n = 0
     for it in range(args.warmup + args.steps):
         n, i_ms = timed_call(stream, ctx.init_disk_photons)
-        if it == 0:
-            q = p.copy()
-            q.nphotons = n
-            ctx.set_params(q)
         st, r_ms = timed_call(stream, ctx.run)
         if it >= args.warmup:
             init_ms += i_ms
@@ -720,7 +723,8 @@ def run_disk(args):
         "emission_ms": init_ms / args.steps, "transport_ms": run_ms / args.steps,
         "rk_steps_per_s": st["accepted_steps"] * args.steps / (total * 1e-3), "packets": n,
         "higher_is_better": True, "dtype": "f64", "data": "synthetic (Fishbone-Moncrief torus)",
-        "config": {"workload": w.name, "grid": "x".join(map(str, w.grid)), "spin": w.spin}}), flush=True)
+        "config": {"workload": w.name, "grid": "x".join(map(str, w.grid)), "spin": w.spin, "launch": cfg}}),
+          flush=True)
 
 
 def main():

@@ -152,7 +152,7 @@ struct grt_ctx {
     DevBuf<unsigned long long> arrived;
     DevBuf<unsigned long long> scratch_u64;
     unsigned long long* host_u64 = nullptr;  // pinned
-    grt_launch_config lc{128, 4, 1, 32, 1};
+    grt_launch_config lc{128, 4, 8, 32, 1};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // images of the last grt_init_image_photons (one, cameras from p) or
     // grt_init_image_batch call; image k owns photon slots

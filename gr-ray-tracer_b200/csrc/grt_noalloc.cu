@@ -269,7 +269,7 @@ extern "C" grt_status grt_trace_device_noalloc(const grt_params* p, const grt_de
     kp.ph.phase = photons->phase;
     kp.n = n;
     kp.counters = counters;
-    kp.refill_threshold = 1;
+    kp.refill_threshold = 8;
     kp.grab = 32;
 
     grt_run_stats st;

@@ -154,15 +154,16 @@ typedef struct grt_image_products {
     uint64_t* arrived_count;      /* [1] */
 } grt_image_products;
 
-/* Launch shape of the trace kernel (chosen by grt_autotune or set by hand). */
+/* Launch shape of the trace kernel: the library's default is {128, 4, 8, 32, 1};
+ * grt/autotune.py times the candidates on a workload and picks one. */
 typedef struct grt_launch_config {
     int32_t threads_per_block;    /* 128 (the trace kernels' block size) */
     int32_t blocks_per_sm;        /* 2, 3 or 4 resident blocks per SM: register caps 255 / 170 / 128 */
     int32_t refill_threshold;     /* idle lanes in a warp before it pulls new photons (1..32) */
     int32_t photons_per_grab;     /* photons a warp claims per access to the global queue */
-    int32_t split_legs;           /* image mode: 1 = trace the backward leg of every ray in one launch and
-                                     the rest in a second (same results, smaller loop bodies); 0 = one
-                                     launch for whole rays */
+    int32_t split_legs;           /* image mode: 1 = the backward legs, the packet generation at first
+                                     fluid contact and the rest as three launches (same results, smaller
+                                     loop bodies); 0 = one launch for whole rays */
 } grt_launch_config;
 
 typedef struct grt_ctx grt_ctx;
