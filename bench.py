@@ -10,7 +10,8 @@ Workload (default, the configuration the headline metric is quoted on):
 Forms, each timed over the same steps:
   fp64           the plain FP64 parity kernel, one 256x256 image per step
                  (initialise the 65,536 pixel rays on the device, trace them
-                 to termination with grt_run, build the image products);
+                 to termination, build the image products), run as the
+                 context's CUDA graph like the batched forms;
   fp64_batched   the same kernel on the C2 image at four frequency channels
                  (230/345/86/43 GHz: custom generator frequency and emission
                  coefficient scaled by f/230 GHz) traced by ONE persistent
@@ -188,6 +189,14 @@ def barrier(world):
         dist.barrier()
 
 
+def max_rel_diff(a, b):
+    """Largest |a - b| / max(|a|, |b|) over the entries (0 where equal)."""
+    import numpy as np
+    scale = np.maximum(np.maximum(np.abs(a), np.abs(b)), 1e-300)
+    d = np.where(a == b, 0.0, np.abs(a - b) / scale)
+    return float(d.max()) if d.size else 0.0
+
+
 def pinned_photons(n):
     """Photon SoA in one pinned (page-locked) host block laid out like the
     library's device block (grt_host_photon_layout), so it moves in one copy."""
@@ -241,13 +250,15 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    # Forms (all on the same torus, all through the C ABI):
-    #   fp64           -- the plain FP64 parity kernel, one image per launch
-    #                     (the reference's structure), grt_run;
+    # Forms (all on the same torus, all through the C ABI, each step one
+    # render through the context's CUDA graph: init the rays, trace them,
+    # build every image's products on the device):
+    #   fp64           -- the plain FP64 parity kernel on one image (one
+    #                     frequency channel), the library's default launch shape;
     #   fp64_batched   -- the FP64 kernel on the batch (every frequency channel
-    #                     of the image in one persistent launch), render graph;
-    #   mixed_batched  -- the mixed FP32/FP64 kernel on the batch, autotuned
-    #                     launch shape, render graph.
+    #                     of the image in one persistent launch);
+    #   mixed_batched  -- the mixed FP32/FP64 kernel on the batch.
+    # The batched forms pick their launch shape with the autotuner.
     FORMS = {"fp64": (abi.PREC_FP64, False), "fp64_batched": (abi.PREC_FP64, True),
              "mixed_batched": (abi.PREC_MIXED, True)}
     wanted = [f for f in args.forms.split(",") if f]
@@ -280,21 +291,13 @@ def run_ours(args):
             cfg[name] = ctx.launch_config()
     peak64, peak32 = lib.measure_fma_peaks()
 
-    def one_step(ctx, batched):
-        if batched:
-            st = ctx.render_graph()  # graph: init rays, trace, every image's products
-            return st, None
-        ctx.init_image_photons(w.pixels, w.pixels)
-        st = ctx.run()
-        return st, ctx.image_products()
-
     results = {}
     images = {}
     sampler = ClockSampler(local).__enter__()
     for name, (ctx, batched) in forms.items():
         prepare(ctx, batched)
         for _ in range(args.warmup):
-            one_step(ctx, batched)
+            ctx.render_graph()  # graph: init rays, trace, every image's products
         torch.cuda.synchronize()
         barrier(world)
         total_ms = 0.0
@@ -307,7 +310,7 @@ def run_ours(args):
                 flush_buf.zero_()
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev0.record(stream)
-            st, prod = one_step(ctx, batched)
+            st = ctx.render_graph()
             ev1.record(stream)
             ev1.synchronize()
             total_ms += ev0.elapsed_time(ev1)
@@ -324,7 +327,7 @@ def run_ours(args):
         if batched:
             images[name] = [ctx.batch_image_products(k).image_I.copy() for k in range(len(specs))]
         else:
-            images[name] = [prod.image_I.copy()]
+            images[name] = [ctx.image_products().image_I.copy()]
         results[name] = dict(ms_per_step=total_ms / args.steps, trace_ms_per_launch=trace_ms / args.steps,
                              stats=stats_acc, launches=launches, rays=n_rays,
                              rays_per_s=world * n_rays * args.steps / (total_ms * 1e-3),
@@ -451,7 +454,8 @@ def run_ours(args):
         host_wall_ms = (time.perf_counter() - t0) * 1e3
         sampler.timed(False)
         e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
-        same_images = all(np.array_equal(outs[c][k].image_I, images[head][k])
+        # per-pixel sums of several arrivals are in atomic order: equal up to rounding
+        diff_images = max(max_rel_diff(outs[c][k].image_I, images[head][k])
                           for c in (0, 1) for k in range(len(specs)))
         ctx2.close()
     sampler.__exit__(None, None, None)
@@ -462,7 +466,7 @@ def run_ours(args):
         e2e = {"value": world * n_rays * args.steps / (e2e_ms * 1e-3), "unit": "rays/s",
                "ms_per_step": e2e_ms / args.steps, "host_wall_ms_per_step": host_wall_ms / args.steps,
                "mode": "streamed: two contexts in turn on one stream (grt_render_async)",
-               "images_equal_value_form": same_images}
+               "image_I_max_rel_diff_vs_value_form": diff_images}
     e2e.update(h2d_bytes_per_step=PHOTON_BYTES * n_rays, d2h_bytes_per_step=d2h)
 
     # ---- roofline of the dominant kernel (the headline form's trace kernel) ----
