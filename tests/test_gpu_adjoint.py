@@ -152,7 +152,7 @@ def test_torch_autograd_function(gpu):
         assert np.allclose(m_abs.grad.numpy(), ga, rtol=1e-6, atol=1e-12 * np.abs(ga).max())
         assert np.allclose(m_emis.grad.numpy(), ge, rtol=1e-6, atol=1e-12 * np.abs(ge).max())
         # a few plain gradient steps lower the loss (step 0.05 L / |grad|^2)
-        first = float(loss)
+        first = float(loss.detach())
         gnorm2 = float(np.sum(ga ** 2) + np.sum(ge ** 2))
         opt = torch.optim.SGD([m_abs, m_emis], lr=0.05 * first / gnorm2)
         for _ in range(5):
