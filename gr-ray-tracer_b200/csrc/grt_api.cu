@@ -388,6 +388,13 @@ const char* grt_build_info(void) {
 
 const char* grt_last_error(const grt_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+// Between grt_render_async and grt_render_wait the context's device buffers
+// belong to the render in flight: calls that would enqueue work on them or
+// read them are refused.
+static grt_status rendering(grt_ctx* c) {
+    return fail(c, GRT_ESTATE, "a render is in flight on this context (grt_render_wait first)");
+}
+
 grt_status grt_create(const grt_params* p, grt_ctx** out) {
     if (!p || !out) return GRT_EINVAL;
     *out = nullptr;
@@ -454,6 +461,7 @@ void grt_destroy(grt_ctx* c) {
 }
 
 grt_status grt_set_params(grt_ctx* c, const grt_params* p) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || !p) return GRT_EINVAL;
     char buf[512];
     if (grt_params_validate(p, buf, sizeof(buf)) != GRT_OK) return fail(c, GRT_EINVAL, buf);
@@ -463,6 +471,7 @@ grt_status grt_set_params(grt_ctx* c, const grt_params* p) {
 }
 
 grt_status grt_set_stream(grt_ctx* c, void* stream) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
     ++c->generation;
@@ -482,6 +491,7 @@ grt_status grt_get_launch_config(const grt_ctx* c, grt_launch_config* cfg) {
 }
 
 grt_status grt_set_launch_config(grt_ctx* c, const grt_launch_config* cfg) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || !cfg) return GRT_EINVAL;
     if (cfg->threads_per_block != 128)
         return fail(c, GRT_EINVAL, "threads_per_block must be 128 (the trace kernels' block size)");
@@ -500,6 +510,7 @@ grt_status grt_set_launch_config(grt_ctx* c, const grt_launch_config* cfg) {
 grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const double* r, const double* th,
                            const double* ph, const double* rho, const double* T, const double* vel4,
                            const double* mag4) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     const size_t ncell = nr * nth * nph;
     ++c->generation;
@@ -599,6 +610,7 @@ grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const 
 }
 
 grt_status grt_upload_grid_numpy_dir(grt_ctx* c, const char* dir) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || !dir) return GRT_EINVAL;
     namespace fs = std::filesystem;
     const fs::path root(dir);
@@ -642,6 +654,7 @@ static grt_status count_initial_terminated(grt_ctx* c) {
 }
 
 grt_status grt_upload_photons(grt_ctx* c, const grt_photon_soa* s, size_t n) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || (!s && n)) return GRT_EINVAL;
     if (n > (1ull << 40)) return fail(c, GRT_EINVAL, "photon count too large");
     const bool keep_images = c->have_images && n == c->n;  // same slots: photons keep their images
@@ -701,6 +714,7 @@ grt_status grt_host_photon_layout(void* block, size_t n, grt_photon_soa* soa) {
 }
 
 grt_status grt_download_photons(grt_ctx* c, grt_photon_soa* s) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || !s) return GRT_EINVAL;
     const size_t n = c->n;
     if (n == 0) return GRT_OK;
@@ -1027,6 +1041,7 @@ int64_t single_launch_steps_done(const grt_params& p, unsigned long long termina
 extern "C" {
 
 grt_status grt_init_image_photons(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t id_offset) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     const grt_image_spec sp = spec_from_params(c->p, nx, ny);
     if (nx * ny == 0) {
@@ -1044,6 +1059,7 @@ grt_status grt_init_image_photons(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t
 
 grt_status grt_init_image_rows(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t row0, uint64_t nrows,
                                uint64_t id_offset) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     if (nx == 0 || ny == 0 || nrows == 0 || row0 >= ny || nrows > ny - row0)
         return fail(c, GRT_EINVAL, "rows [row0, row0 + nrows) must lie inside the ny-row screen");
@@ -1053,6 +1069,7 @@ grt_status grt_init_image_rows(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t ro
 
 grt_status grt_init_image_forward_photons(grt_ctx* c, uint64_t nx, uint64_t ny, double back_distance,
                                           uint64_t id_offset) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     if (!(back_distance > 0.0) || !std::isfinite(back_distance))
         return fail(c, GRT_EINVAL, "back_distance must be positive");
@@ -1062,6 +1079,7 @@ grt_status grt_init_image_forward_photons(grt_ctx* c, uint64_t nx, uint64_t ny, 
 }
 
 grt_status grt_init_disk_photons(grt_ctx* c, uint64_t id_offset, uint64_t* n_photons) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     if (!c->grid_uploaded || !c->fluid_available)
         return fail(c, GRT_ESTATE, "disk emission needs an uploaded fluid grid");
@@ -1124,6 +1142,7 @@ grt_status grt_init_disk_photons(grt_ctx* c, uint64_t id_offset, uint64_t* n_pho
 }
 
 grt_status grt_init_image_batch(grt_ctx* c, const grt_image_spec* specs, size_t nimages, uint64_t id_offset) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     if (!specs || nimages == 0) return fail(c, GRT_EINVAL, "an image batch needs at least one image");
     if (nimages > (1u << 20)) return fail(c, GRT_EINVAL, "too many images in one batch");
@@ -1133,6 +1152,7 @@ grt_status grt_init_image_batch(grt_ctx* c, const grt_image_spec* specs, size_t 
 size_t grt_batch_image_count(const grt_ctx* c) { return c && c->batched ? c->images.size() : 0; }
 
 grt_status grt_set_channel_sharing(grt_ctx* c, int enable) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     c->share_channels = enable != 0;
     ++c->generation;
@@ -1173,6 +1193,7 @@ static grt_status ensure_batch_products(grt_ctx* c) {
 }
 
 grt_status grt_get_batch_image_products(grt_ctx* c, size_t image, grt_image_products* out) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || !out) return GRT_EINVAL;
     grt_status st = ensure_batch_products(c);
     if (st != GRT_OK) return st;
@@ -1184,6 +1205,7 @@ grt_status grt_get_batch_image_products(grt_ctx* c, size_t image, grt_image_prod
 }
 
 grt_status grt_get_all_batch_image_products(grt_ctx* c, grt_image_products* outs, size_t nimages) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || (!outs && nimages)) return GRT_EINVAL;
     grt_status st = ensure_batch_products(c);
     if (st != GRT_OK) return st;
@@ -1308,11 +1330,13 @@ grt_status run_steps(grt_ctx* c, grt_run_stats* stats, const OutputPlan* plan) {
 extern "C" {
 
 grt_status grt_run(grt_ctx* c, grt_run_stats* stats) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     return run_steps(c, stats, nullptr);
 }
 
 grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     if (!c->grid_uploaded) return fail(c, GRT_ESTATE, "grt_render_graph before grt_upload_grid");
     if (!c->have_images) return fail(c, GRT_ESTATE, "grt_render_graph needs grt_init_image_photons or grt_init_image_batch");
@@ -1506,6 +1530,7 @@ grt_status grt_render_wait(grt_ctx* c, grt_run_stats* stats) {
 }
 
 grt_status grt_set_cell_multipliers(grt_ctx* c, const double* m_abs, const double* m_emis) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     const size_t ncell = static_cast<size_t>(c->nr) * c->nth * c->nph;
     if ((m_abs || m_emis) && (!c->grid_uploaded || !c->fluid_available || ncell == 0))
@@ -1527,6 +1552,7 @@ grt_status grt_set_cell_multipliers(grt_ctx* c, const double* m_abs, const doubl
 }
 
 grt_status grt_forward_checkpointed(grt_ctx* c, int64_t K, grt_run_stats* stats) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     if (!c->grid_uploaded) return fail(c, GRT_ESTATE, "grt_forward_checkpointed before grt_upload_grid");
     const grt_params& p = c->p;
@@ -1597,6 +1623,7 @@ grt_status grt_forward_checkpointed(grt_ctx* c, int64_t K, grt_run_stats* stats)
 }
 
 grt_status grt_adjoint_image_I(grt_ctx* c, const double* dL_dI, double* g_abs, double* g_emis) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || !dL_dI) return GRT_EINVAL;
     if (!c->adj_ready) return fail(c, GRT_ESTATE, "grt_adjoint_image_I needs a grt_forward_checkpointed first");
     if (c->batched) return fail(c, GRT_EINVAL, "the adjoint covers single-image runs");
@@ -1650,6 +1677,7 @@ grt_status grt_adjoint_image_I(grt_ctx* c, const double* dL_dI, double* g_abs, d
 }
 
 grt_status grt_get_image_products(grt_ctx* c, grt_image_products* out) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || !out) return GRT_EINVAL;
     const grt_params& p = c->p;
     const size_t npix = p.image_nx * p.image_ny, bins = p.spectrum_bins;
@@ -1807,6 +1835,7 @@ grt_status make_output_plan(grt_ctx* c, const char* output_dir, const char* name
 extern "C" {
 
 grt_status grt_write_image_products_npz(grt_ctx* c, const char* output_dir, const char* name) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || !output_dir || !name) return GRT_EINVAL;
     const grt_params& p = c->p;
     const size_t nx = p.image_nx, ny = p.image_ny, bins = p.spectrum_bins;
@@ -1819,6 +1848,7 @@ grt_status grt_write_image_products_npz(grt_ctx* c, const char* output_dir, cons
 }
 
 grt_status grt_write_batch_products_npz(grt_ctx* c, const char* output_dir, const char* name) {
+    if (c && c->render_pending) return rendering(c);
     if (!c || !output_dir || !name) return GRT_EINVAL;
     if (!c->batched) return fail(c, GRT_ESTATE, "no image batch (grt_init_image_batch)");
     const size_t bins = c->p.spectrum_bins;
@@ -1839,6 +1869,7 @@ grt_status grt_write_batch_products_npz(grt_ctx* c, const char* output_dir, cons
 
 grt_status grt_write_output_step_npz(grt_ctx* c, const char* output_dir, const char* name, int64_t step,
                                      int32_t rank, const char* variables, uint64_t stride) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     OutputPlan plan;
     const grt_status ps = make_output_plan(c, output_dir, name, variables, stride, rank, plan);
@@ -1848,6 +1879,7 @@ grt_status grt_write_output_step_npz(grt_ctx* c, const char* output_dir, const c
 
 grt_status grt_run_with_output(grt_ctx* c, const char* output_dir, const char* name, const char* variables,
                                uint64_t stride, grt_run_stats* stats) {
+    if (c && c->render_pending) return rendering(c);
     if (!c) return GRT_EINVAL;
     OutputPlan plan;
     grt_status s = make_output_plan(c, output_dir, name, variables, stride, c->p.rank, plan);

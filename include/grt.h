@@ -428,7 +428,8 @@ grt_status grt_render_graph(grt_ctx* ctx, grt_run_stats* stats);
  * The batch keeps its images, as grt_upload_photons with the batch's count
  * does.  Needs an image batch and termination_percent >= 1.  The host buffers
  * must stay untouched until grt_render_wait returns; one render is in flight
- * per context (GRT_ESTATE otherwise).  Two contexts given the same stream
+ * per context, and until its grt_render_wait every other call on the context
+ * that sets it up, enqueues work or reads results returns GRT_ESTATE.  Two contexts given the same stream
  * (grt_set_stream) and used in turn keep their traces in order on it while
  * one's copies overlap the other's trace.  grt_render_wait blocks until the
  * render's products are on the host and fills stats as grt_run does.

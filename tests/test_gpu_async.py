@@ -155,8 +155,17 @@ def test_async_render_errors(gpu):
         with pytest.raises(GrtError) as e:
             ctx.render_async(x, outs)
         assert e.value.status == abi.GRT_ESTATE
+        # the render in flight owns the context's device buffers: other work is refused until the wait
+        for call in (ctx.run, lambda: ctx.upload_photons(x), ctx.download_photons, ctx.render_graph,
+                     lambda: ctx.batch_image_products(0), lambda: ctx.init_image_batch(specs)):
+            with pytest.raises(GrtError) as e:
+                call()
+            assert e.value.status == abi.GRT_ESTATE
         st = ctx.render_wait()
         assert st["n_terminated"] == x.n
+        # and accepted again after it
+        ctx.upload_photons(x)
+        assert ctx.run()["n_terminated"] == x.n
     finally:
         ctx.close()
     # a single image (grt_init_image_photons) is not a batch
