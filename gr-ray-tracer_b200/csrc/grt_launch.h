@@ -136,10 +136,11 @@ inline int rcp_params_ok(double a, double M) {
     return a_ok && m_ok ? 1 : 0;
 }
 
-// Dynamic shared memory of a trace launch: k1..k5 slots for RK45 (5*7 doubles
-// per thread) plus the separable axes and their half-spans (2*(nr+nth+nph)).
+// Dynamic shared memory of a trace launch: the stage slots for RK45 (6*7
+// doubles per thread: k1..k5, then the state) plus the separable axes and
+// their half-spans (2*(nr+nth+nph)).
 inline size_t dev_trace_smem_bytes(int integrator, int threads, bool separable, int nr, int nth, int nph) {
-    size_t n = integrator == 1 ? static_cast<size_t>(5 * 7) * threads : 0;
+    size_t n = integrator == 1 ? static_cast<size_t>(6 * 7) * threads : 0;
     if (separable) n += 2 * static_cast<size_t>(nr + nth + nph);
     return n * sizeof(double);
 }

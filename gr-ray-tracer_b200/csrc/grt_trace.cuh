@@ -241,11 +241,13 @@ static __constant__ double kFehlbergA[5][5] = {
 // __launch_bounds__ use the same constant).
 constexpr int kTraceThreads = 128;
 
-// Per-thread slots for the stage derivatives k1..k5 in shared memory:
-// [5][7][kTraceThreads] doubles, thread-contiguous so a warp's accesses are
-// conflict-free; base already points at this thread's column, so a slot is a
-// constant offset from it.  k1 stays there across the retries of one call.
-constexpr int kStageSlots = 5;
+// Per-thread slots in shared memory: the stage derivatives k1..k5 (slots
+// 0..4; k6 replaces k2 in slot 1 once the last stage input is formed) and the
+// state (slot 5) for the error norm.  [6][7][kTraceThreads] doubles,
+// thread-contiguous so a warp's accesses are conflict-free; base already
+// points at this thread's column, so a slot is a constant offset from it.
+// k1 stays there across the retries of one call.
+constexpr int kStageSlots = 6;
 struct KStore {
     double* base;
     GRT_DEV double& at(int j, int c) const { return base[(j * 7 + c) * kTraceThreads]; }
@@ -260,14 +262,18 @@ static __device__ __noinline__ double controller_root(double x) { return fourth_
 // if accepted (s advanced), 0 if rejected; *dl receives the next proposed step
 // either way.  All right-hand sides go through one site in a rolled stage
 // loop -- a lane that needs k1 runs it one iteration ahead of the others, so
-// the warp stays converged on the same code -- and k1..k5 live in shared
-// memory (slots 0..4), which keeps registers for the right-hand side.  Each stage input is summed over j = 1..t-1 left to right, the
-// reference's association; for the first stage, dt*(a21 k1) equals the
-// reference's (dt*a21)*k1 because a21 = 1/4 is a power of two.
+// the warp stays converged on the same code -- and the derivatives live in
+// shared memory (KStore), which keeps registers for the right-hand side.
+// The stage sums and the error norm are rolled loops too, the norm with a
+// single division site: every inline IEEE division brings its slow path into
+// the step loop's instruction stream, and with seven of them unrolled the
+// loop missed the instruction cache far more (the unrolled form was 11-22%
+// slower on C2 and C3).  Each stage input is summed over j = 1..t-1 left to
+// right, the reference's association; for the first stage, dt*(a21 k1)
+// equals the reference's (dt*a21)*k1 because a21 = 1/4 is a power of two.
 template <class RHS>
 GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, int need_k1, int fast, const KStore& kk) {
     const double dt = *dl;
-    V7 k6;
     double t[8];
     t[4] = s[4];
 #pragma unroll 1
@@ -280,38 +286,38 @@ GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, int need_k1
             const double a0 = kFehlbergA[st][0];
 #pragma unroll
             for (int c = 0; c < 7; ++c) acc[c] = a0 * kk.at(0, c);
+#pragma unroll 1
+            for (int j = 1; j <= st; ++j) {
+                const double aj = kFehlbergA[st][j];
 #pragma unroll
-            for (int j = 1; j <= 4; ++j) {
-                if (j <= st) {
-                    const double aj = kFehlbergA[st][j];
-#pragma unroll
-                    for (int c = 0; c < 7; ++c) acc[c] = acc[c] + aj * kk.at(j, c);
-                }
+                for (int c = 0; c < 7; ++c) acc[c] = acc[c] + aj * kk.at(j, c);
             }
 #pragma unroll
             for (int c = 0; c < 7; ++c) t[sidx(c)] = s[sidx(c)] + dt * acc[c];
         }
         const V7 k = RHS::eval(t, kp, fast);
-        if (st < 4) {
+        // k2..k5 to slots 1..4; k6 replaces k2 in slot 1 (no later use)
+        const int slot = st < 4 ? st + 1 : 1;
 #pragma unroll
-            for (int c = 0; c < 7; ++c) kk.at(st + 1, c) = k.v[c];
-        } else {
-            k6 = k;
-        }
+        for (int c = 0; c < 7; ++c) kk.at(slot, c) = k.v[c];
     }
-    double x5[7];
+    // The state goes to slot 5 so that the error norm runs as a loop over the
+    // components (one division site); x5 replaces it there.
+#pragma unroll
+    for (int c = 0; c < 7; ++c) kk.at(5, c) = s[sidx(c)];
     double err = 0.0;
     bool finite = isfinite(s[4]);
-#pragma unroll
+#pragma unroll 1
     for (int c = 0; c < 7; ++c) {
-        const double si = s[sidx(c)];
-        const double k1 = kk.at(0, c), k3 = kk.at(2, c), k4 = kk.at(3, c), k5 = kk.at(4, c);
+        const double si = kk.at(5, c);
+        const double k1 = kk.at(0, c), k3 = kk.at(2, c), k4 = kk.at(3, c), k5 = kk.at(4, c), k6 = kk.at(1, c);
         const double x4 = si + dt * (b41 * k1 + b43 * k3 + b44 * k4 + b45 * k5);
-        x5[c] = si + dt * (b51 * k1 + b53 * k3 + b54 * k4 + b55 * k5 + b56 * k6.v[c]);
-        const double sc = kp.atol + kp.rtol * fmax(fabs(x5[c]), fabs(x4));
-        const double ratio = fabs(x5[c] - x4) / sc;
-        if (!isfinite(x5[c]) || !isfinite(ratio)) finite = false;
+        const double x5 = si + dt * (b51 * k1 + b53 * k3 + b54 * k4 + b55 * k5 + b56 * k6);
+        const double sc = kp.atol + kp.rtol * fmax(fabs(x5), fabs(x4));
+        const double ratio = fabs(x5 - x4) / sc;
+        if (!isfinite(x5) || !isfinite(ratio)) finite = false;
         err = fmax(err, ratio);
+        kk.at(5, c) = x5;
     }
     if (!finite) {
         *dl = dt * kp.min_scale;
@@ -320,7 +326,7 @@ GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, int need_k1
     if (err == 0.0) {
         *dl = dt * kp.max_scale;
 #pragma unroll
-        for (int c = 0; c < 7; ++c) s[sidx(c)] = x5[c];
+        for (int c = 0; c < 7; ++c) s[sidx(c)] = kk.at(5, c);
         return 1;
     }
     double scale = kp.safety * controller_root(1.0 / err);
@@ -328,7 +334,7 @@ GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, int need_k1
     *dl = dt * scale;
     if (err <= 1.0) {
 #pragma unroll
-        for (int c = 0; c < 7; ++c) s[sidx(c)] = x5[c];
+        for (int c = 0; c < 7; ++c) s[sidx(c)] = kk.at(5, c);
         return 1;
     }
     return 0;
@@ -881,7 +887,7 @@ GRT_DEV void generate_body(const KParams& kp, const Axes& ax) {
     }
 }
 
-// Shared-memory layout of a trace block: [k2..k5 slots (RK45)] [axes and
+// Shared-memory layout of a trace block: [stage slots (RK45)] [axes and
 // half-spans of a separable grid].  Returns the staged pointers.
 GRT_DEV void stage_grid(const KParams& kp, double* smem, int integrator, Axes& ax, KStore& kk) {
     const KGrid& G = kp.grid;
