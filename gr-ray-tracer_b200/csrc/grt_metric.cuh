@@ -34,8 +34,15 @@ struct Rhs7 {
 GRT_DEV double ks_radius(double x, double y, double z, double a) {
     const double rsq = x * x + y * y + z * z;
     const double A = rsq - a * a;
-    const double S = sqrt(A * A + 4.0 * ((a * z) * (a * z)));
-    return sqrt(0.5 * (A + S));
+    double r = A * A + 4.0 * ((a * z) * (a * z));
+    // S = sqrt(A^2 + 4 (a z)^2), then r = sqrt((A + S) / 2), through one
+    // sqrt site (a rolled loop keeps the step loop's code small)
+#pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+        const double v = sqrt(r);
+        r = k == 0 ? 0.5 * (A + v) : v;
+    }
+    return r;
 }
 
 // kerr_schild_core.hpp:157-192 (with compute_r_and_deriv :36-46,
@@ -100,8 +107,9 @@ GRT_DEV Rhs7 ks_rhs(double x, double y, double z, double pt, double px, double p
 }
 
 // ks_rhs with every quotient formed from the correctly rounded reciprocal of
-// its denominator (six of them: S, 2r, B, r, D, D^2) by div_by, which rounds
-// like an IEEE division while no value under- or overflows.  That holds in
+// its denominator (six of them: S, 2r, B, r, D, D^2; five reciprocal
+// evaluations, since RN(1/(2r)) = RN(1/r) / 2) by div_by, which rounds like an
+// IEEE division while no value under- or overflows.  That holds in
 // the box this checks first: x, y, z each an exact zero or of magnitude in
 // [2^-20, 2^20], r in [2^-24, 2^20] and S in [2^-60, 2^42], with a spin of
 // magnitude 0 or in [2^-20, 2] and a mass in [2^-20, 2^20] (checked on the
@@ -115,8 +123,19 @@ GRT_DEV Rhs7 ks_rhs_rcp(double x, double y, double z, double pt, double px, doub
                         double a, double M, bool& ok) {
     const double rsq = x * x + y * y + z * z;
     const double A = rsq - a * a;
-    const double S = sqrt(A * A + 4.0 * ((a * z) * (a * z)));
-    const double r = sqrt(0.5 * (A + S));
+    // S = sqrt(A^2 + 4 (a z)^2), then r = sqrt((A + S) / 2), through one sqrt
+    // site as in ks_radius
+    double S = 0.0, r = A * A + 4.0 * ((a * z) * (a * z));
+#pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+        const double v = sqrt(r);
+        if (k == 0) {
+            S = v;
+            r = 0.5 * (A + S);
+        } else {
+            r = v;
+        }
+    }
     ok = div_zero_or_within<-20, 19>(x) && div_zero_or_within<-20, 19>(y) && div_zero_or_within<-20, 19>(z) &&
          div_within<-24, 19>(r) && div_within<-60, 41>(S);
     Rhs7 o{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -124,13 +143,15 @@ GRT_DEV Rhs7 ks_rhs_rcp(double x, double y, double z, double pt, double px, doub
     const double yS = div_recip(S);
     const double opas = 1.0 + div_by(A, S, yS);
     const double two_r = 2.0 * r;
-    const double y2r = div_recip(two_r);
+    // RN(1/(2r)) = RN(1/r) / 2 exactly: r is inside the box, so no rounding
+    // step under- or overflows
+    const double yr = div_recip(r);
+    const double y2r = 0.5 * yr;
     const double dr0 = div_by(x * opas, two_r, y2r);
     const double dr1 = div_by(y * opas, two_r, y2r);
     const double dr2 = div_by(z * opas + div_by(2.0 * (a * a) * z, S, yS), two_r, y2r);
     const double B = r * r + a * a;
     const double yB = div_recip(B);
-    const double yr = div_recip(r);
     const double l1 = div_by(r * x + a * y, B, yB);
     const double l2 = div_by(r * y - a * x, B, yB);
     const double l3 = div_by(z, r, yr);

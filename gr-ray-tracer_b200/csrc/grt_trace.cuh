@@ -329,7 +329,9 @@ GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, int need_k1
         for (int c = 0; c < 7; ++c) s[sidx(c)] = kk.at(5, c);
         return 1;
     }
-    double scale = kp.safety * controller_root(1.0 / err);
+    // 1/err rounded to nearest, as the division 1.0 / err rounds it (err is
+    // finite and positive here), without a second division site
+    double scale = kp.safety * controller_root(div_recip(err));
     scale = fmin(kp.max_scale, fmax(kp.min_scale, scale));
     *dl = dt * scale;
     if (err <= 1.0) {
