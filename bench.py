@@ -246,6 +246,9 @@ def run_ours(args):
     world, rank, local = dist_setup(args.gpus)
     w = workloads.WORKLOADS[args.workload]
     bw = workloads.BATCHES[args.workload]
+    if args.images:
+        # a slice of the batch (its first N images), for profiling runs
+        bw = workloads.BatchWorkload(f"{bw.name}_first{args.images}", bw.base, bw.images[:args.images])
     grid = w.torus()
     stream = torch.cuda.Stream()
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -283,7 +286,12 @@ def run_ours(args):
     # FP64 form keeps the library's default shape
     cfg = {}
     for name, (ctx, batched) in forms.items():
-        if batched and not args.no_autotune:
+        if batched and args.launch:
+            b, r, g, sp = (int(v) for v in args.launch.split(","))
+            ctx.set_launch_config(threads_per_block=128, blocks_per_sm=b, refill_threshold=r,
+                                  photons_per_grab=g, split_legs=sp)
+            cfg[name] = ctx.launch_config()
+        elif batched and not args.no_autotune:
             cfg[name], _, table = autotune.tune(ctx, lambda c: prepare(c, True), bw.name, log=None)
             for c, ms in sorted(table, key=lambda x: x[1])[:4]:
                 log(f"autotune {name} {c} {ms:.3f} ms")
@@ -743,6 +751,11 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="use the library's default launch shape")
     ap.add_argument("--forms", default="fp64,fp64_batched,mixed_batched",
                     help="comma list of fp64, fp64_batched, mixed_batched")
+    ap.add_argument("--images", type=int, default=0,
+                    help="only the first N images of the workload's batch (a slice for profiling)")
+    ap.add_argument("--launch", default="",
+                    help="fixed launch shape of the batched forms: blocks_per_sm,refill_threshold,"
+                         "photons_per_grab,split_legs (instead of the autotuner)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
     if args.impl == "reference":
