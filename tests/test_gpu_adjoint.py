@@ -160,7 +160,7 @@ def test_torch_autograd_function(gpu):
             l2 = ((r.render(m_abs, m_emis).float() - target) ** 2).sum()
             l2.backward()
             opt.step()
-        final = float(((r.render(m_abs, m_emis).float() - target) ** 2).sum())
+        final = float(((r.render(m_abs, m_emis).float() - target) ** 2).sum().detach())
         assert final < first
     finally:
         r.close()
