@@ -706,6 +706,10 @@ def run_disk(args):
     if rank != 0:  # a one-GPU measurement: rank 0 runs it, the other ranks exit
         return
     w = workloads.C5
+    if args.disk_normalization:
+        # fewer packets (a smaller case of the same run, for profiling)
+        w = workloads.DiskWorkload(f"{w.name}_norm{args.disk_normalization:g}", w.grid, w.spin,
+                                   args.disk_normalization)
     p = w.params()
     stream = torch.cuda.Stream()
     ctx = lib.Context(p)
@@ -715,7 +719,11 @@ def run_disk(args):
     q = p.copy()
     q.nphotons = n
     ctx.set_params(q)
-    if not args.no_autotune:
+    if args.launch:
+        b, r, g, sp = (int(v) for v in args.launch.split(","))
+        ctx.set_launch_config(threads_per_block=128, blocks_per_sm=b, refill_threshold=r, photons_per_grab=g,
+                              split_legs=sp)
+    elif not args.no_autotune:
         from grt import autotune
         autotune.tune(ctx, lambda c: c.init_disk_photons(), w.name, reps=1)
     cfg = ctx.launch_config()
@@ -754,8 +762,11 @@ def main():
     ap.add_argument("--images", type=int, default=0,
                     help="only the first N images of the workload's batch (a slice for profiling)")
     ap.add_argument("--launch", default="",
-                    help="fixed launch shape of the batched forms: blocks_per_sm,refill_threshold,"
+                    help="fixed launch shape of the batched forms (and of c5): blocks_per_sm,refill_threshold,"
                          "photons_per_grab,split_legs (instead of the autotuner)")
+    ap.add_argument("--disk-normalization", type=float, default=0.0,
+                    help="c5 only: superphoton normalisation (packets per unit density) instead of the "
+                         "workload's 210, e.g. 21 for about 1e6 packets (a smaller case for profiling)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
     if args.impl == "reference":

@@ -136,6 +136,28 @@ GRT_DEV int nearest_azimuth_sorted(const double* ph, int n, double az) {
 GRT_DEV bool within_radial_sorted(const double* r, const double* half, int i, double radius) {
     return fabs(log(radius / r[i])) <= half[i];
 }
+
+// nearest_radial_sorted and within_radial_sorted in one pass: the log
+// distance of the chosen cell is the one the nearest-cell test computed, so it
+// is evaluated once per candidate (one or two), through one site.  Ties go to
+// the lower index, as in nearest_radial_sorted.
+GRT_DEV bool locate_radial_sorted(const double* r, const double* half, int n, double radius, int& i) {
+    const int lo = bracket(r, n, radius);
+    const int c0 = lo < 0 ? 0 : lo;
+    const int ncand = (lo >= 0 && lo + 1 < n) ? 2 : 1;
+    double best = 0.0;
+    int bi = c0;
+#pragma unroll 1
+    for (int k = 0; k < ncand; ++k) {
+        const double d = fabs(log(radius / r[c0 + k]));
+        if (k == 0 || d < best) {
+            best = d;
+            bi = c0 + k;
+        }
+    }
+    i = bi;
+    return best <= half[bi];
+}
 GRT_DEV bool within_polar_sorted(const double* th, const double* half, int j, double polar) {
     return fabs(polar - th[j]) <= half[j];
 }
@@ -253,13 +275,15 @@ GRT_DEV bool build_tetrad(const double g[4][4], const double u[4], double e[4][4
     const double ts = u[0] >= 0.0 ? 1.0 : -1.0;
 #pragma unroll
     for (int mu = 0; mu < 4; ++mu) e[0][mu] = ts * u[mu] * inv;
-#pragma unroll
+    // Rolled over the spatial axes (one square-root and one division site):
+    // the tetrad is built on every fluid sample, so its code stays small.
+#pragma unroll 1
     for (int axis = 0; axis < 3; ++axis) {
         double cand[4];
         const double tp = metric_dot_unit(g, e[0], axis + 1);
 #pragma unroll
         for (int mu = 0; mu < 4; ++mu) cand[mu] = (mu == axis + 1 ? 1.0 : 0.0) + tp * e[0][mu];
-#pragma unroll
+#pragma unroll 1
         for (int prev = 0; prev < axis; ++prev) {
             const double proj = metric_dot(g, e[prev + 1], cand);
 #pragma unroll
@@ -318,8 +342,7 @@ static __device__ __noinline__ bool sample_fluid_at(const KParams& kp, const Axe
     const KGrid& G = kp.grid;
     int i, j, k;
     if (G.separable) {
-        i = nearest_radial_sorted(ax.r, G.nr, radius);
-        if (!within_radial_sorted(ax.r, ax.rh, i, radius)) return false;
+        if (!locate_radial_sorted(ax.r, ax.rh, G.nr, radius, i)) return false;
     }
     const double ct = fmax(-1.0, fmin(1.0, s[3] / radius));
     const double polar = acos(ct);
