@@ -1005,8 +1005,11 @@ grt_status prepare_trace_buffers(grt_ctx* c, unsigned long long queue) {
 cudaError_t launch_trace(const grt_ctx* c, const grt::KParams& kp, size_t smem) {
     const grt_params& p = c->p;
     const bool mixed = p.precision == GRT_PREC_MIXED;
-    if (!split_legs(c))
-        return grt::launch_trace(kp, mixed, 0, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+    if (!split_legs(c)) {
+        // disk mode: the whole-ray kernel without the image-mode code (leg 3)
+        const int leg = p.mode == GRT_MODE_DISK && kp.ngroups == 0 ? 3 : 0;
+        return grt::launch_trace(kp, mixed, leg, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+    }
     cudaError_t e = cudaMemsetAsync(kp.calls_carry, 0, kp.n * sizeof(long long), c->stream);
     if (e == cudaSuccess)
         e = grt::launch_trace(kp, mixed, 1, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);

@@ -249,13 +249,15 @@ cudaError_t launch_gather_fields(const GatherArgs& a, int sm_count, cudaStream_t
 cudaError_t launch_trace(const KParams& kp, bool mixed, int leg, int integrator, int sm_count, int blocks_per_sm,
                          size_t smem, cudaStream_t stream) {
     const int blocks = sm_count * blocks_per_sm;
-    switch (leg + (mixed ? 3 : 0)) {
+    switch (leg + (mixed ? 4 : 0)) {
         case 0: return launch_trace_fp64_leg0(kp, integrator, blocks_per_sm, blocks, smem, stream);
         case 1: return launch_trace_fp64_leg1(kp, integrator, blocks_per_sm, blocks, smem, stream);
         case 2: return launch_trace_fp64_leg2(kp, integrator, blocks_per_sm, blocks, smem, stream);
-        case 3: return launch_trace_mixed_leg0(kp, integrator, blocks_per_sm, blocks, smem, stream);
-        case 4: return launch_trace_mixed_leg1(kp, integrator, blocks_per_sm, blocks, smem, stream);
-        case 5: return launch_trace_mixed_leg2(kp, integrator, blocks_per_sm, blocks, smem, stream);
+        case 3: return launch_trace_fp64_leg3(kp, integrator, blocks_per_sm, blocks, smem, stream);
+        case 4: return launch_trace_mixed_leg0(kp, integrator, blocks_per_sm, blocks, smem, stream);
+        case 5: return launch_trace_mixed_leg1(kp, integrator, blocks_per_sm, blocks, smem, stream);
+        case 6: return launch_trace_mixed_leg2(kp, integrator, blocks_per_sm, blocks, smem, stream);
+        case 7: return launch_trace_mixed_leg3(kp, integrator, blocks_per_sm, blocks, smem, stream);
         default: return cudaErrorInvalidConfiguration;
     }
 }

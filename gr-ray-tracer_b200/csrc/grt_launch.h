@@ -154,7 +154,7 @@ cudaError_t launch_adjoint_reverse(const KParams& kp, const AdjointArgs& aa, int
 // Persistent trace launches (grt_trace_inst.cu): `blocks` blocks of 128
 // threads; blocks_per_sm in {2, 3, 4} picks the register cap (255 / 170 /
 // 128); leg 0 traces whole rays, legs 1 and 2 the backward leg and the rest
-// of image-mode rays (trace_body).
+// of image-mode rays, leg 3 whole disk-mode rays (trace_body).
 cudaError_t launch_trace_fp64_leg0(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
                                    cudaStream_t stream);
 cudaError_t launch_trace_fp64_leg1(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
@@ -166,6 +166,10 @@ cudaError_t launch_trace_mixed_leg0(const KParams& kp, int integrator, int block
 cudaError_t launch_trace_mixed_leg1(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
                                     cudaStream_t stream);
 cudaError_t launch_trace_mixed_leg2(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
+                                    cudaStream_t stream);
+cudaError_t launch_trace_fp64_leg3(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
+                                   cudaStream_t stream);
+cudaError_t launch_trace_mixed_leg3(const KParams& kp, int integrator, int blocks_per_sm, int blocks, size_t smem,
                                     cudaStream_t stream);
 // Packet generation between the backward-leg and forward-leg launches
 // (photons with calls_carry < 0), one thread per queue index; smem holds the

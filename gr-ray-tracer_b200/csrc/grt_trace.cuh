@@ -481,11 +481,13 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
     L.radius = ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
     L.have_radius = 1;
     const bool backward = phase0 == 1;  // ImageBackward
-    const bool needs = kp.scat_on || kp.abs_on || kp.emis_on || (kp.image_mode && backward);
+    // LEG 3 (disk mode) compiles the image-mode branches out of the step loop
+    const bool image_mode = LEG != 3 && kp.image_mode;
+    const bool needs = kp.scat_on || kp.abs_on || kp.emis_on || (image_mode && backward);
     FluidSample fs;
     const bool sampled = needs && sample_fluid<RAW>(kp, ax, L.s, L.radius, fs);
     int terminated = 0;
-    if (LEG != 2 && kp.image_mode && backward && sampled) {
+    if (LEG != 2 && image_mode && backward && sampled) {
         if (LEG == 1) {
             // the backward-leg launch stops here: generate_body samples
             // this position again and generates (one call, split)
@@ -551,7 +553,7 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
         }
         rec.rt_step(fs.cell, tau0, j0, I_before, att, scale);
     }
-    if (LEG != 1 && kp.image_mode && phase0 == 2) {  // ImageForward
+    if (LEG != 1 && image_mode && phase0 == 2) {  // ImageForward
         double u = 0.0, v = 0.0;
         const int crossing = camera_crossing(im, L.s, u, v);
         if (crossing > 0) {
@@ -608,7 +610,10 @@ GRT_DEV void store_carry(const KParams& kp, const Lane& L) {
 //      in KParams::calls_carry[q] (negated: -(calls + 1), generation pending);
 //      generate_body then finishes those calls, one thread per photon;
 //   2  everything after: photons in any live phase but ImageBackward,
-//      resuming with the calls left in calls_carry[q].
+//      resuming with the calls left in calls_carry[q];
+//   3  disk mode: whole rays like 0, with the image-mode branches (packet
+//      generation at first contact, camera arrival) compiled out, which keeps
+//      the step loop's code small for the instruction cache.
 // Each photon takes the same calls in the same order either way, so the split
 // launches give the one-launch result bit for bit; each loop body holds only
 // its own leg's code.
@@ -679,7 +684,7 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                         slot = chan_slot(kp, lo, L.lead, L.pix);
                     }
                     if (q >= 0 && !kp.ph.terminate[slot] &&
-                        (LEG == 0 || ((kp.ph.phase[slot] == 1) == (LEG == 1)))) {
+                        (LEG == 0 || LEG == 3 || ((kp.ph.phase[slot] == 1) == (LEG == 1)))) {
                         load_photon<LEG == 1>(kp.ph, slot, L);
                         L.idx = slot;
                         L.q = q;

@@ -1,13 +1,14 @@
 // Persistent trace kernels of one precision form and one leg.  The Makefile
-// compiles this file six times, with GRT_MIXED in {0, 1} and GRT_LEG in
-// {0, 1, 2}, all with -fmad=false so that every product and sum rounds
+// compiles this file eight times, with GRT_MIXED in {0, 1} and GRT_LEG in
+// {0, 1, 2, 3}, all with -fmad=false so that every product and sum rounds
 // separately, as in the reference's host build:
 //   trace_fp64<I,B,SHARE,LEG>   FP64 parity form (integrate_cart_ks.hpp:230-419)
 //   trace_mixed<I,B,SHARE,LEG>  mixed FP32/FP64 form (grt_rhs_mixed.cuh)
 // I = integrator (0 RK4, 1 RK45); B = resident 128-thread blocks per SM, which
 // caps the registers per thread at 65536 / (128 * B): 255, 170, 128 for
 // B = 2, 3, 4; SHARE = frequency channels share one geodesic; LEG = whole
-// rays (0), the backward leg (1) or the rest (2) of image-mode rays.
+// rays (0), the backward leg (1) or the rest (2) of image-mode rays, or
+// whole disk-mode rays without the image-mode code (3).
 #include "grt_launch.h"
 #include "grt_trace.cuh"
 
@@ -38,11 +39,16 @@ namespace {
 
 template <int I, int B>
 cudaError_t launch_v(const KParams& kp, int blocks, size_t smem, cudaStream_t stream) {
-    if (kp.ngroups > 0) {
+    if constexpr (GRT_LEG == 3) {
+        // disk mode never shares channels
+        if (kp.ngroups > 0) return cudaErrorInvalidValue;
+    } else if (kp.ngroups > 0) {
         cudaFuncSetAttribute(GRT_TRACE_KERNEL<I, B, true, GRT_LEG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
         GRT_TRACE_KERNEL<I, B, true, GRT_LEG><<<blocks, 128, smem, stream>>>(kp);
-    } else {
+        return cudaGetLastError();
+    }
+    {
         cudaFuncSetAttribute(GRT_TRACE_KERNEL<I, B, false, GRT_LEG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
         GRT_TRACE_KERNEL<I, B, false, GRT_LEG><<<blocks, 128, smem, stream>>>(kp);
