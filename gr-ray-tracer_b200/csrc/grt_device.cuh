@@ -415,24 +415,32 @@ constexpr double kProtonMassCgs = 1.67262192369e-24;   // scattering.hpp:256
 constexpr double kSigmaThomsonCgs = 6.6524587158e-25;  // scattering.hpp:257
 
 // State a scattering event may change, passed by copy to the out-of-line
-// maybe_scatter so the caller's state never has its address taken (which would
-// keep it in local memory for the whole trace loop).
+// scatter_packet so the caller's state never has its address taken (which
+// would keep it in local memory for the whole trace loop).
 struct ScatterState {
     double s[8];
     double I[4];
 };
 
-// maybe_scatter_photon (scattering.hpp:259-313); st is changed only when it
-// returns true.
-static __device__ __noinline__ bool maybe_scatter(ScatterState* st, double albedo, double dl, double length_scale,
-                           const FluidSample& fs, double a, double M, Philox& rng) {
-    double* s = st->s;
-    double* I = st->I;
+// maybe_scatter_photon (scattering.hpp:259-313) in two parts.  scatter_drawn is the
+// part every sampled step takes, inline: the Thomson optical depth over the
+// proposed step and the first draw; it says whether the packet scatters.
+GRT_DEV bool scatter_drawn(double dl, double length_scale, const FluidSample& fs, Philox& rng) {
     const double path_cm = dl * length_scale;
     const double ne = fs.fluid.density_g_cm3 / kProtonMassCgs;
     const double tau = kSigmaThomsonCgs * ne * path_cm;
     const double prob = 1.0 - exp(-tau);
-    if (rng.drand() >= prob) return false;
+    return !(rng.drand() >= prob);  // the reference's rejection test, NaN included
+}
+
+// The rest, out of line and only for a packet that scatters: the isotropic
+// fluid-frame direction (two more draws), the new covariant momentum and the
+// albedo weights; false leaves the state as it was.
+static __device__ __noinline__ bool scatter_packet(ScatterState* st, double albedo, const FluidSample& fs, double a,
+                                                   double M, Philox* rngp) {
+    Philox& rng = *rngp;
+    double* s = st->s;
+    double* I = st->I;
     double E = 0.0;
 #pragma unroll
     for (int mu = 0; mu < 4; ++mu) E -= s[4 + mu] * fs.e[0][mu];

@@ -538,17 +538,19 @@ GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, do
         }
         if (kp.scat_on) {
             Philox rng(kp.seed, L.id, static_cast<uint32_t>(step));
-            ScatterState st;
+            if (scatter_drawn(fabs(L.dl), kp.length_scale, fs, rng)) {
+                ScatterState st;
 #pragma unroll
-            for (int c = 0; c < 8; ++c) st.s[c] = L.s[c];
+                for (int c = 0; c < 8; ++c) st.s[c] = L.s[c];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) st.I[q] = L.I[q];
-            if (maybe_scatter(&st, kp.albedo, fabs(L.dl), kp.length_scale, fs, kp.a, kp.M, rng)) {
+                for (int q = 0; q < 4; ++q) st.I[q] = L.I[q];
+                if (scatter_packet(&st, kp.albedo, fs, kp.a, kp.M, &rng)) {
 #pragma unroll
-                for (int c = 4; c < 8; ++c) L.s[c] = st.s[c];
+                    for (int c = 4; c < 8; ++c) L.s[c] = st.s[c];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) L.I[q] = st.I[q];
-                scale = kp.albedo;
+                    for (int q = 0; q < 4; ++q) L.I[q] = st.I[q];
+                    scale = kp.albedo;
+                }
             }
         }
         rec.rt_step(fs.cell, tau0, j0, I_before, att, scale);
