@@ -285,7 +285,7 @@ bool well_separated_increasing(const std::vector<double>& a) {
 }
 
 // Shared memory a trace block may spend on staged separable axes (the RK45
-// stage slots take 35 KB of the 227 KB a block can have).
+// stage slots take 42 KB of the 227 KB a block can have).
 constexpr size_t kMaxStagedAxisBytes = 160 * 1024;
 
 grt::KParams make_kparams(const grt_ctx* c) {
