@@ -337,7 +337,8 @@ def run_ours(args):
         else:
             images[name] = [ctx.image_products().image_I.copy()]
         results[name] = dict(ms_per_step=total_ms / args.steps, trace_ms_per_launch=trace_ms / args.steps,
-                             stats=stats_acc, launches=launches, rays=n_rays,
+                             stats=stats_acc, launches=launches, rays=n_rays, geodesics=ctx.geodesics,
+                             geodesics_per_s=world * ctx.geodesics * args.steps / (total_ms * 1e-3),
                              rays_per_s=world * n_rays * args.steps / (total_ms * 1e-3),
                              rk_steps_per_s=world * stats_acc["accepted_steps"] * args.steps / (total_ms * 1e-3))
 
@@ -500,6 +501,10 @@ def run_ours(args):
             "value": H["rays_per_s"],
             "unit": "rays/s",
             "rk_steps_per_s": H["rk_steps_per_s"],
+            # one traced geodesic carries every frequency channel of its pixel
+            # (channel sharing), so rays/s counts channel images and
+            # geodesics_per_s counts traced geodesics
+            "geodesics_per_s": H["geodesics_per_s"],
             "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup,
@@ -516,16 +521,28 @@ def run_ours(args):
                        "grid": "x".join(map(str, w.grid)), "spin": w.spin, "inclination_deg": w.inclination_deg,
                        "integrator": "rk45" if w.integrator else "rk4", "rtol": w.rtol,
                        "headline_form": head, "launch": cfg.get(head),
+                       "rays_per_step": H["rays"], "geodesics_per_step": H["geodesics"],
+                       "channel_sharing": bool(batched and H["geodesics"] < H["rays"]),
                        "l2": "flushed by a 256 MB device write before every timed step (outside the events)",
                        "parallelism": f"replicas x{world}"},
             "forms": {k: {"rays_per_step": v["rays"], "rays_per_s": v["rays_per_s"],
+                          "geodesics_per_step": v["geodesics"], "geodesics_per_s": v["geodesics_per_s"],
                           "rk_steps_per_s": v["rk_steps_per_s"],
                           "ms_per_step": v["ms_per_step"], "trace_ms_per_launch": v["trace_ms_per_launch"],
                           "accepted_steps": v["stats"]["accepted_steps"],
                           "rejected_attempts": v["stats"]["rejected_attempts"],
                           "launch": cfg.get(k)} for k, v in results.items()},
+            # where the speed-up comes from: batching with channel sharing
+            # (rays per traced geodesic) and the precision form at equal
+            # geodesics (mixed batch against the FP64 batch, trace only)
             "speedup_mixed_batched_vs_fp64": (results["mixed_batched"]["rays_per_s"] / results["fp64"]["rays_per_s"]
                                               if "mixed_batched" in results and "fp64" in results else None),
+            "speedup_mixed_vs_fp64_same_batch": (
+                results["fp64_batched"]["trace_ms_per_launch"] / results["mixed_batched"]["trace_ms_per_launch"]
+                if "mixed_batched" in results and "fp64_batched" in results else None),
+            "speedup_fp64_batched_vs_fp64_per_geodesic": (
+                results["fp64_batched"]["geodesics_per_s"] / results["fp64"]["geodesics_per_s"]
+                if "fp64_batched" in results and "fp64" in results else None),
             "stokes_I_rel_err": stokes_err,
             "stokes_I_max_pixel_rel_err": per_pixel,
             "e2e": e2e,
@@ -565,7 +582,6 @@ def cpu_baseline(w, reps=2, params=None, label=None):
                     best = (st["elapsed_s"], st["stepped"])
         else:
             o = pyoracle.Oracle()
-            o.set_pow_mode("libm")
             kind = "port"
             for _ in range(reps):
                 ph = o.init_image_photons(p, w.pixels, w.pixels)

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "grt.h"
+#include "grt_grid_axes.h"
 #include "grt_host.h"
 #include "grt_kparams.h"
 #include "grt_launch.h"
@@ -27,7 +28,6 @@
 
 namespace {
 
-constexpr double kPi = 3.14159265358979323846;
 
 template <class T>
 struct DevBuf {
@@ -152,7 +152,7 @@ struct grt_ctx {
     DevBuf<unsigned long long> arrived;
     DevBuf<unsigned long long> scratch_u64;
     unsigned long long* host_u64 = nullptr;  // pinned
-    grt_launch_config lc{128, 4, 8, 32, 1};
+    grt_launch_config lc{128, 4, 8, 32, 1, 0, 0};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // images of the last grt_init_image_photons (one, cameras from p) or
     // grt_init_image_batch call; image k owns photon slots
@@ -161,6 +161,7 @@ struct grt_ctx {
     std::vector<unsigned long long> image_start;
     uint64_t image_id_offset = 0;
     double forward_back = 0.0;  // > 0: line-of-sight forward rays from -forward_back * n
+    bool random_screen = false;  // image rays at the reference's random screen positions
     uint64_t row0 = 0, nrows = 0;  // single image: pixel rows [row0, row0 + nrows) only (nrows 0 = all)
     bool batched = false;      // trace kernels read the per-image table
     bool have_images = false;  // photons came from an image init (a render can re-initialise them)
@@ -242,46 +243,6 @@ void spherical_to_cartesian_vec(double r, double th, double ph, double spin, con
     c[2] = radial_y * s[1] + theta_y * s[2] + phi_y * s[3];
     c[3] = radial_z * s[1] + theta_z * s[2];
     for (int q = 0; q < 4; ++q) c[q] *= scale;
-}
-
-// scattering.hpp:99-149: the acceptance half-width 0.500001 * (largest
-// neighbour span) of each separable axis value, evaluated with glibc like the
-// reference evaluates it on every call.
-double periodic_distance(double lhs, double rhs) {
-    const double d = std::fmod(std::fabs(lhs - rhs), 2.0 * kPi);
-    return std::fmin(d, 2.0 * kPi - d);
-}
-std::vector<double> half_spans(const std::vector<double>& a, int kind) {
-    const size_t n = a.size();
-    std::vector<double> h(n);
-    for (size_t i = 0; i < n; ++i) {
-        if (n == 1) {
-            h[i] = 1.0e-10;
-            continue;
-        }
-        double span = 0.0;
-        for (int side = 0; side < 2; ++side) {
-            if ((side == 0 && i == 0) || (side == 1 && i + 1 >= n)) continue;
-            const double nb = a[side == 0 ? i - 1 : i + 1];
-            double d;
-            if (kind == 0) d = std::fabs(std::log(a[i] / nb));
-            else if (kind == 1) d = std::fabs(a[i] - nb);
-            else d = periodic_distance(a[i], nb);
-            span = std::fmax(span, d);
-        }
-        h[i] = 0.500001 * span;
-    }
-    return h;
-}
-
-bool well_separated_increasing(const std::vector<double>& a) {
-    for (size_t i = 1; i < a.size(); ++i) {
-        if (!(a[i] > a[i - 1])) return false;
-        const double gap = a[i] - a[i - 1];
-        const double mag = std::max(std::fabs(a[i]), std::fabs(a[i - 1]));
-        if (!(gap > 1e-12 * mag)) return false;
-    }
-    return true;
 }
 
 // Shared memory a trace block may spend on staged separable axes (the RK45
@@ -502,7 +463,9 @@ grt_status grt_set_launch_config(grt_ctx* c, const grt_launch_config* cfg) {
     if (cfg->photons_per_grab < 1 || cfg->photons_per_grab > (1 << 20))
         return fail(c, GRT_EINVAL, "photons_per_grab must be in [1, 2^20]");
     if (cfg->split_legs != 0 && cfg->split_legs != 1) return fail(c, GRT_EINVAL, "split_legs must be 0 or 1");
+    if (cfg->max_iterations < 0) return fail(c, GRT_EINVAL, "max_iterations must be >= 0 (0 = automatic)");
     c->lc = *cfg;
+    c->lc.pad = 0;
     ++c->generation;
     return GRT_OK;
 }
@@ -538,8 +501,7 @@ grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const 
                 const size_t q = (i * nth + j) * nph + k;
                 if (!(r[q] == ra[i]) || !(th[q] == ta[j]) || !(ph[q] == pa[k])) sep = false;
             }
-    sep = sep && well_separated_increasing(ra) && well_separated_increasing(ta) &&
-          well_separated_increasing(pa) && ra[0] > 0.0 && pa[0] >= 0.0 && pa[nph - 1] < 2.0 * kPi;
+    sep = sep && grt::axes::axes_stageable(ra.data(), nr, ta.data(), nth, pa.data(), nph);
     // the staged axes and half-spans (16 bytes per axis value) must fit in
     // shared memory beside the RK45 stage slots; longer axes use the general
     // lookup on the full coordinate arrays
@@ -549,12 +511,7 @@ grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const 
     // 0.6 > 0.500001 of the outermost log spacing), so lookup can stop early.
     c->r_reject_lo = 0.0;
     c->r_reject_hi = INFINITY;
-    if (sep && nr >= 2) {
-        const double span_lo = std::fabs(std::log(ra[0] / ra[1]));
-        const double span_hi = std::fabs(std::log(ra[nr - 1] / ra[nr - 2]));
-        c->r_reject_lo = ra[0] * std::exp(-0.6 * span_lo);
-        c->r_reject_hi = ra[nr - 1] * std::exp(0.6 * span_hi);
-    }
+    if (sep) grt::axes::radial_reject_bounds(ra.data(), nr, &c->r_reject_lo, &c->r_reject_hi);
     std::vector<double2> rt(ncell), uv(2 * ncell), bv(2 * ncell);
     std::vector<double> pos(3 * ncell);
     c->host_rho.assign(rho, rho + ncell);
@@ -589,7 +546,10 @@ grt_status grt_upload_grid(grt_ctx* c, size_t nr, size_t nth, size_t nph, const 
     GRT_CUDA(c, cudaMemcpy(c->th_axis.ptr, ta.data(), nth * sizeof(double), cudaMemcpyHostToDevice), "H2D axis");
     GRT_CUDA(c, cudaMemcpy(c->ph_axis.ptr, pa.data(), nph * sizeof(double), cudaMemcpyHostToDevice), "H2D axis");
     if (sep) {
-        const std::vector<double> rh = half_spans(ra, 0), th_h = half_spans(ta, 1), ph_h = half_spans(pa, 2);
+        std::vector<double> rh(nr), th_h(nth), ph_h(nph);
+        grt::axes::half_spans(ra.data(), nr, 0, rh.data());
+        grt::axes::half_spans(ta.data(), nth, 1, th_h.data());
+        grt::axes::half_spans(pa.data(), nph, 2, ph_h.data());
         GRT_CUDA(c, c->r_half.alloc(nr), "alloc half");
         GRT_CUDA(c, c->th_half.alloc(nth), "alloc half");
         GRT_CUDA(c, c->ph_half.alloc(nph), "alloc half");
@@ -697,6 +657,12 @@ grt_status grt_upload_photons(grt_ctx* c, const grt_photon_soa* s, size_t n) {
 
 size_t grt_photon_count(const grt_ctx* c) { return c ? c->n : 0; }
 
+uint64_t grt_geodesic_count(const grt_ctx* c) {
+    if (!c) return 0;
+    const bool scat = c->p.scattering_enabled && c->fluid_available;
+    return c->batched && c->share_channels && c->groups_share && !scat ? c->geodesics : c->n;
+}
+
 size_t grt_photon_block_bytes(size_t n) { return 146 * n; }
 
 grt_status grt_host_photon_layout(void* block, size_t n, grt_photon_soa* soa) {
@@ -796,13 +762,17 @@ grt_status launch_image_inits(grt_ctx* c) {
             a.dlambda0 = p.initial_step * B;
             a.nu0 = sp.custom_frequency_hz;
         }
+        // initialize_photons.hpp:115: the random pool is seeded 12345 + rank
+        a.random_screen = c->random_screen ? 1 : 0;
+        a.seed = 12345ull + static_cast<unsigned long long>(static_cast<long long>(p.rank));
         GRT_CUDA(c, grt::launch_init_image(a, c->stream), "init_image_pixels");
     }
     return GRT_OK;
 }
 
 grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages, uint64_t id_offset, bool batched,
-                         double forward_back = 0.0, uint64_t row0 = 0, uint64_t nrows = 0) {
+                         double forward_back = 0.0, uint64_t row0 = 0, uint64_t nrows = 0,
+                         bool random_screen = false) {
     unsigned long long total = 0;
     std::vector<unsigned long long> start(nimages + 1, 0);
     for (size_t k = 0; k < nimages; ++k) {
@@ -826,6 +796,7 @@ grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages
     c->image_start = start;
     c->image_id_offset = id_offset;
     c->forward_back = forward_back;
+    c->random_screen = random_screen;
     c->row0 = row0;
     c->nrows = nrows;
     c->batched = batched;
@@ -979,7 +950,12 @@ void fill_spectrum_frequencies(const grt_params& p, double* out) {
 
 // Per-warp loop limit of a trace launch (GRT_ETIMEOUT beyond it): every
 // photon may take `budget` calls of at most 13 attempts each.
-unsigned long long iteration_limit(const grt::KParams& kp, unsigned long long total, int blocks, int threads) {
+// Per-warp loop limit of a trace launch: the launch shape's max_iterations
+// when set, else a bound no launch that makes progress reaches (every warp
+// iteration is one RK45 attempt or RK4 step of at least one lane).
+unsigned long long iteration_limit(const grt_ctx* c, const grt::KParams& kp, unsigned long long total, int blocks,
+                                   int threads) {
+    if (c->lc.max_iterations > 0) return static_cast<unsigned long long>(c->lc.max_iterations);
     const unsigned long long warps = static_cast<unsigned long long>(blocks) * (threads / 32);
     return static_cast<unsigned long long>(kp.budget + 2) * 13ull *
                ((total + warps - 1) / warps + static_cast<unsigned long long>(kp.grab)) +
@@ -1058,6 +1034,16 @@ grt_status grt_init_image_photons(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t
         return GRT_OK;
     }
     return set_image_set(c, &sp, 1, id_offset, false);
+}
+
+grt_status grt_init_image_photons_random(grt_ctx* c, uint64_t n, uint64_t id_offset) {
+    if (c && c->render_pending) return rendering(c);
+    if (!c) return GRT_EINVAL;
+    if (n == 0) return grt_init_image_photons(c, 0, 0, id_offset);
+    // one row of n rays: the slot layout only; products bin by arrival (u, v)
+    // into output.image_nx x image_ny
+    const grt_image_spec sp = spec_from_params(c->p, n, 1);
+    return set_image_set(c, &sp, 1, id_offset, false, 0.0, 0, 0, true);
 }
 
 grt_status grt_init_image_rows(grt_ctx* c, uint64_t nx, uint64_t ny, uint64_t row0, uint64_t nrows,
@@ -1285,7 +1271,7 @@ grt_status run_steps(grt_ctx* c, grt_run_stats* stats, const OutputPlan* plan) {
         }
         kp.step0 = step;
         kp.budget = end - step;
-        kp.max_iterations = iteration_limit(kp, total, blocks, threads);
+        kp.max_iterations = iteration_limit(c, kp, total, blocks, threads);
         GRT_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, sizeof(grt::KCounters), c->stream), "memset counters");
         GRT_CUDA(c, cudaEventRecord(c->ev0, c->stream), "event");
         cudaError_t e = launch_trace(c, kp, smem);
@@ -1306,8 +1292,10 @@ grt_status run_steps(grt_ctx* c, grt_run_stats* stats, const OutputPlan* plan) {
         if (k.max_term_step > max_term_step) max_term_step = k.max_term_step;
         if (k.timed_out) {
             st.timed_out = 1;
+            st.steps_done = steps_done;
             st.trace_ms = ms_total;
             st.n_terminated = terminated;
+            c->initial_terminated = terminated;  // a later run continues these photons
             if (stats) *stats = st;
             return fail(c, GRT_ETIMEOUT, "trace kernel hit its iteration limit");
         }
@@ -1324,6 +1312,7 @@ grt_status run_steps(grt_ctx* c, grt_run_stats* stats, const OutputPlan* plan) {
     st.steps_done = steps_done;
     st.n_terminated = terminated;
     st.trace_ms = ms_total;
+    c->initial_terminated = terminated;
     if (stats) *stats = st;
     return GRT_OK;
 }
@@ -1366,7 +1355,7 @@ grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
         }
         kp.step0 = 0;
         kp.budget = p.max_steps;
-        kp.max_iterations = iteration_limit(kp, c->n, c->sm_count * c->lc.blocks_per_sm, 128);
+        kp.max_iterations = iteration_limit(c, kp, c->n, c->sm_count * c->lc.blocks_per_sm, 128);
         const size_t smem = trace_smem(c);
         GRT_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed), "begin capture");
         grt_status gs = launch_image_inits(c);
@@ -1430,7 +1419,7 @@ static grt_status enqueue_render(grt_ctx* c, const grt_photon_soa* s, grt_image_
     kp.calls_carry = c->calls_carry.ptr;
     kp.step0 = 0;
     kp.budget = c->p.max_steps;
-    kp.max_iterations = iteration_limit(kp, n, c->sm_count * c->lc.blocks_per_sm, 128);
+    kp.max_iterations = iteration_limit(c, kp, n, c->sm_count * c->lc.blocks_per_sm, 128);
     GRT_CUDA(c, cudaMemcpyAsync(c->ph.block.ptr, s->id, grt_photon_block_bytes(n), cudaMemcpyHostToDevice,
                                 c->copy_stream), "H2D photons");
     GRT_CUDA(c, cudaEventRecord(c->ev_uploaded, c->copy_stream), "event");
@@ -1732,7 +1721,7 @@ grt_status write_products_archive(grt_ctx* c, const std::string& output_dir, con
     ok = z.close() && ok;
     if (!ok) {
         fs::remove(tmp, ec);
-        return fail(c, GRT_EIO, "Failed while writing NumPy archive");
+        return fail(c, GRT_EIO, z.error().empty() ? std::string("Failed while writing NumPy archive") : z.error());
     }
     fs::rename(tmp, final_path, ec);
     if (ec) {
@@ -1806,7 +1795,7 @@ grt_status write_output_step(grt_ctx* c, const OutputPlan& plan, int64_t step) {
     ok = z.close() && ok;
     if (!ok) {
         fs::remove(tmp, ec);
-        return fail(c, GRT_EIO, "Failed while writing NumPy archive");
+        return fail(c, GRT_EIO, z.error().empty() ? std::string("Failed while writing NumPy archive") : z.error());
     }
     fs::rename(tmp, final_path, ec);
     if (ec) {

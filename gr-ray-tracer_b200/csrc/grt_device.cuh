@@ -64,7 +64,8 @@ struct Philox {
         return static_cast<double>((hi << 21) | (lo >> 11)) * (1.0 / 9007199254740992.0);
     }
 };
-constexpr uint32_t kInitDomain = 0xFFFFFFFFu;
+constexpr uint32_t kInitDomain = 0xFFFFFFFFu;    // disk-mode emission draws
+constexpr uint32_t kScreenDomain = 0xFFFFFFFEu;  // image-mode random screen (u, v)
 
 // ---------------------------------------------------------------------------
 // Nonuniform (r, theta, phi) grid lookup (scattering.hpp:41-180)

@@ -534,11 +534,20 @@ bool NpzOut::open(const std::string& path) {
     out_.open(path, std::ios::binary | std::ios::trunc);
     offset_ = 0;
     entries_.clear();
+    error_.clear();
+    if (!out_) error_ = "Failed to open output NumPy archive: " + path;
     return static_cast<bool>(out_);
 }
 
+// The archive is a stored (uncompressed) ZIP without the ZIP64 extension, as
+// the reference writes it (cnpy.h:176-181, 220-248): sizes and offsets are
+// 32-bit fields, so an archive that outgrows them is refused, not wrapped.
 bool NpzOut::add(const std::string& name, const std::vector<char>& payload) {
     const std::string member = name + ".npy";
+    if (member.size() > 0xffffu || payload.size() > limit_ || offset_ > limit_) {
+        error_ = "NumPy archive exceeds the non-ZIP64 size limit";
+        return false;
+    }
     Entry e{member, crc32_of(payload), static_cast<uint32_t>(payload.size()), static_cast<uint32_t>(offset_)};
     std::vector<char> h;
     put32(h, 0x04034b50u);
@@ -551,10 +560,16 @@ bool NpzOut::add(const std::string& name, const std::vector<char>& payload) {
     out_.write(payload.data(), static_cast<std::streamsize>(payload.size()));
     offset_ += h.size() + member.size() + payload.size();
     entries_.push_back(e);
+    if (!out_) error_ = "Failed while writing NumPy archive";
     return static_cast<bool>(out_);
 }
 
 bool NpzOut::close() {
+    if (entries_.size() > 0xffffu) {
+        error_ = "NumPy archive contains too many arrays";
+        out_.close();
+        return false;
+    }
     const uint64_t cd_offset = offset_;
     for (const Entry& e : entries_) {
         std::vector<char> h;
@@ -569,6 +584,11 @@ bool NpzOut::close() {
         out_.write(e.name.data(), static_cast<std::streamsize>(e.name.size()));
         offset_ += h.size() + e.name.size();
     }
+    if (cd_offset > limit_ || offset_ - cd_offset > limit_) {
+        error_ = "NumPy archive exceeds the non-ZIP64 size limit";
+        out_.close();
+        return false;
+    }
     std::vector<char> end;
     put32(end, 0x06054b50u);
     put16(end, 0); put16(end, 0);
@@ -579,6 +599,7 @@ bool NpzOut::close() {
     put16(end, 0);
     out_.write(end.data(), static_cast<std::streamsize>(end.size()));
     out_.close();
+    if (!out_ && error_.empty()) error_ = "Failed while writing NumPy archive";
     return static_cast<bool>(out_);
 }
 

@@ -31,9 +31,14 @@ bool parse_output_variables(const std::string& spec, std::vector<int>& fields, s
 // Uncompressed (STORED) .npz writer.
 class NpzOut {
 public:
+    // limit: the largest member, member offset and central directory a
+    // non-ZIP64 archive can describe (32-bit fields); smaller only in tests
+    explicit NpzOut(uint64_t limit = 0xffffffffull) : limit_(limit) {}
     bool open(const std::string& path);
     bool add(const std::string& name, const std::vector<char>& payload);
     bool close();
+    // why add() or close() failed ("" when they did not)
+    const std::string& error() const { return error_; }
 
 private:
     struct Entry {
@@ -45,6 +50,8 @@ private:
     std::ofstream out_;
     std::vector<Entry> entries_;
     uint64_t offset_ = 0;
+    uint64_t limit_;
+    std::string error_;
 };
 
 }  // namespace grt

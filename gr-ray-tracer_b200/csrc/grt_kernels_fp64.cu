@@ -13,15 +13,26 @@
 
 namespace grt {
 
-// initialize_photons.hpp:116-169 with screen (u, v) at pixel centres; the
-// camera centre and basis come from the host (glibc sin/cos, like the reference).
-// With args.forward, line-of-sight forward rays instead (see InitImageArgs).
+// initialize_photons.hpp:116-169 with screen (u, v) at pixel centres, or
+// with args.random_screen at the reference's uniform random screen position
+// (:123-125, drand(lo, hi) = lo + (hi - lo) d) from Philox keyed by (seed,
+// photon id); the camera centre and basis come from the host (glibc sin/cos,
+// like the reference).  With args.forward, line-of-sight forward rays instead
+// (see InitImageArgs).
 __global__ void init_image_pixels(const __grid_constant__ InitImageArgs args) {
     const unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
     if (i >= args.nx * args.nrows) return;
     const unsigned long long iy = args.row0 + i / args.nx, ix = i % args.nx;
-    const double u = -0.5 * args.W + (static_cast<double>(ix) + 0.5) * args.W / static_cast<double>(args.nx);
-    const double v = -0.5 * args.H + (static_cast<double>(iy) + 0.5) * args.H / static_cast<double>(args.ny);
+    const unsigned long long id = args.id_offset + args.row0 * args.nx + i;
+    double u, v;
+    if (args.random_screen) {
+        dev::Philox rng(args.seed, id, dev::kScreenDomain);
+        u = -0.5 * args.W + args.W * rng.drand();
+        v = -0.5 * args.H + args.H * rng.drand();
+    } else {
+        u = -0.5 * args.W + (static_cast<double>(ix) + 0.5) * args.W / static_cast<double>(args.nx);
+        v = -0.5 * args.H + (static_cast<double>(iy) + 0.5) * args.H / static_cast<double>(args.ny);
+    }
     const bool fwd = args.forward != 0;
     const double x = (fwd ? args.bx : args.cx) + u * args.th_hat[0] + v * args.ph_hat[0];
     const double y = (fwd ? args.by : args.cy) + u * args.th_hat[1] + v * args.ph_hat[1];
@@ -37,7 +48,7 @@ __global__ void init_image_pixels(const __grid_constant__ InitImageArgs args) {
     dev::ks_null_momentum(X, K, args.a, args.M, p);
     const KPhotons& P = args.ph;
     const unsigned long long o = args.offset + i;
-    P.id[o] = args.id_offset + args.row0 * args.nx + i;
+    P.id[o] = id;
     P.frequency[o] = fwd ? args.nu0 : 0.0;
     P.emission_frame_energy[o] = fwd ? -p[0] : 1.0;
     P.x0[o] = 0.0; P.x1[o] = x; P.x2[o] = y; P.x3[o] = z;

@@ -27,6 +27,10 @@ struct InitImageArgs {
     int forward;
     double bx, by, bz;             // -back * n
     double nu0;
+    // the reference's random screen instead of pixel centres: (u, v) from
+    // Philox keyed by (seed, photon id), see kScreenDomain
+    int random_screen;
+    unsigned long long seed;
 };
 
 // initialize_photons_disk (initialize_photons.hpp:173-327): one photon per

@@ -9,7 +9,8 @@
 //
 // The only scratch the trace needs beyond its inputs and outputs -- the work
 // queue head and launch counters, plus the separable grid axes and lookup
-// bounds derived from the coordinate arrays -- lives in one file-scope
+// bounds derived from the coordinate arrays (the bounds on the host, with the
+// routine the context entry point uses, from a static host buffer) -- lives in one file-scope
 // __device__ array of kNoallocScratchBytes (128 KiB) that every GPU which loads
 // this library holds until the process exits.  All calls share it: each call
 // clears the parts that must start at zero, and calls that overlap on the GPU
@@ -24,6 +25,7 @@
 #include <mutex>
 
 #include "grt.h"
+#include "grt_grid_axes.h"
 #include "grt_kparams.h"
 #include "grt_launch.h"
 #include "grt_trace.cuh"
@@ -49,6 +51,11 @@ struct GridMeta {
 std::mutex g_setup_mutex;
 void* g_scratch_addr[kMaxDevices] = {nullptr};
 
+// Host copy of the staged axes and their half-spans while a call derives
+// them (a static buffer: nothing is allocated on the host either).
+std::mutex g_stage_mutex;
+double g_stage_host[2 * kMaxAxisValues];
+
 // Device address of g_noalloc_scratch on the current device (set-up once per device).
 cudaError_t scratch_address(void** out) {
     int dev = 0;
@@ -66,72 +73,27 @@ cudaError_t scratch_address(void** out) {
     return cudaSuccess;
 }
 
-// Separability test and axis staging on the device, one block: the same
-// conditions the host checks in grt_upload_grid (per-axis products, strictly
-// increasing with 1e-12 relative separation, r > 0, phi in [0, 2 pi)).
-__global__ void noalloc_prepare_grid(const double* r, const double* th, const double* ph, int nr, int nth, int nph,
-                                     double* axes, GridMeta* meta) {
-    __shared__ int ok;
-    if (threadIdx.x == 0) ok = 1;
-    __syncthreads();
+// Separability test over every cell, many blocks: a cell whose coordinates
+// differ from the outer product of the axes clears meta->separable (set to all
+// ones before the launch).  Block 0 also copies the three axes into the
+// scratch, from where the host reads them to derive the acceptance bounds.
+__global__ void noalloc_check_grid(const double* r, const double* th, const double* ph, int nr, int nth, int nph,
+                                   double* axes, GridMeta* meta) {
     const long long ncell = static_cast<long long>(nr) * nth * nph;
-    for (long long q = threadIdx.x; q < ncell; q += blockDim.x) {
-        const int k = static_cast<int>(q % nph);
-        const int j = static_cast<int>((q / nph) % nth);
-        const int i = static_cast<int>(q / (static_cast<long long>(nph) * nth));
-        if (!(r[q] == r[static_cast<long long>(i) * nth * nph]) || !(th[q] == th[static_cast<long long>(j) * nph]) ||
-            !(ph[q] == ph[k]))
-            ok = 0;
+    const long long plane = static_cast<long long>(nth) * nph;
+    bool ok = true;
+    for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < ncell;
+         q += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long i = q / plane;
+        const long long j = (q / nph) % nth;
+        const long long k = q % nph;
+        if (!(r[q] == r[i * plane]) || !(th[q] == th[j * nph]) || !(ph[q] == ph[k])) ok = false;
     }
-    double* ra = axes;
-    double* ta = ra + nr;
-    double* pa = ta + nth;
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) ra[i] = r[static_cast<long long>(i) * nth * nph];
-    for (int j = threadIdx.x; j < nth; j += blockDim.x) ta[j] = th[static_cast<long long>(j) * nph];
-    for (int k = threadIdx.x; k < nph; k += blockDim.x) pa[k] = ph[k];
-    __syncthreads();
-    // acceptance half-widths (scattering.hpp:99-149), as the host computes them
-    double* rh = pa + nph;
-    double* thh = rh + nr;
-    double* phh = thh + nth;
-    for (int q = threadIdx.x; q < nr + nth + nph; q += blockDim.x) {
-        const double* a;
-        double* h;
-        int n, i, kind;
-        if (q < nr) { a = ra; h = rh; n = nr; i = q; kind = 0; }
-        else if (q < nr + nth) { a = ta; h = thh; n = nth; i = q - nr; kind = 1; }
-        else { a = pa; h = phh; n = nph; i = q - nr - nth; kind = 2; }
-        double span = 0.0;
-        for (int side = 0; side < 2; ++side) {
-            if ((side == 0 && i == 0) || (side == 1 && i + 1 >= n)) continue;
-            const double nb = a[side == 0 ? i - 1 : i + 1];
-            const double d = kind == 0 ? fabs(log(a[i] / nb)) : kind == 1 ? fabs(a[i] - nb)
-                                                                          : grt::dev::periodic_angle_distance(a[i], nb);
-            span = fmax(span, d);
-        }
-        h[i] = n == 1 ? 1.0e-10 : 0.500001 * span;
-    }
-    __syncthreads();
-    auto separated = [](const double* a, int n, int t) {
-        for (int q = t + 1; q < n; q += blockDim.x) {
-            if (!(a[q] > a[q - 1])) return false;
-            const double gap = a[q] - a[q - 1];
-            const double mag = fmax(fabs(a[q]), fabs(a[q - 1]));
-            if (!(gap > 1e-12 * mag)) return false;
-        }
-        return true;
-    };
-    if (!separated(ra, nr, threadIdx.x) || !separated(ta, nth, threadIdx.x) || !separated(pa, nph, threadIdx.x)) ok = 0;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const bool sep = ok && ra[0] > 0.0 && pa[0] >= 0.0 && pa[nph - 1] < 2.0 * grt::dev::kPi;
-        meta->separable = sep ? 1 : 0;
-        meta->r_reject_lo = 0.0;
-        meta->r_reject_hi = INFINITY;
-        if (sep && nr >= 2) {
-            meta->r_reject_lo = ra[0] * exp(-0.6 * fabs(log(ra[0] / ra[1])));
-            meta->r_reject_hi = ra[nr - 1] * exp(0.6 * fabs(log(ra[nr - 1] / ra[nr - 2])));
-        }
+    if (__any_sync(0xFFFFFFFFu, !ok) && (threadIdx.x & 31) == 0) atomicAnd(&meta->separable, 0);
+    if (blockIdx.x == 0) {
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) axes[i] = r[static_cast<long long>(i) * plane];
+        for (int j = threadIdx.x; j < nth; j += blockDim.x) axes[nr + j] = th[static_cast<long long>(j) * nph];
+        for (int k = threadIdx.x; k < nph; k += blockDim.x) axes[nr + nth + k] = ph[k];
     }
 }
 
@@ -194,12 +156,45 @@ extern "C" grt_status grt_trace_device_noalloc(const grt_params* p, const grt_de
     std::memset(&kp, 0, sizeof(kp));
     GridMeta gm{0, 0, 0.0, INFINITY};
     if (ncell) {
-        noalloc_prepare_grid<<<1, 256, 0, stream>>>(grid->r, grid->theta, grid->phi, static_cast<int>(nr),
-                                                   static_cast<int>(nth), static_cast<int>(nph), axes, meta);
-        cudaError_t e = cudaGetLastError();
+        // 1. the cell-by-cell separability check and the axes, on the device
+        int sms_prep = 148, dev_prep = 0;
+        cudaGetDevice(&dev_prep);
+        cudaDeviceGetAttribute(&sms_prep, cudaDevAttrMultiProcessorCount, dev_prep);
+        const unsigned long long want_blocks = (ncell + 255) / 256;
+        const unsigned blocks = static_cast<unsigned>(
+            want_blocks < static_cast<unsigned long long>(sms_prep) * 8 ? want_blocks : sms_prep * 8ull);
+        cudaError_t e = cudaMemsetAsync(&meta->separable, 0xFF, sizeof(int), stream);
+        if (e == cudaSuccess) {
+            noalloc_check_grid<<<blocks, 256, 0, stream>>>(grid->r, grid->theta, grid->phi, static_cast<int>(nr),
+                                                           static_cast<int>(nth), static_cast<int>(nph), axes, meta);
+            e = cudaGetLastError();
+        }
         if (e == cudaSuccess) e = cudaMemcpyAsync(&gm, meta, sizeof(gm), cudaMemcpyDeviceToHost, stream);
+        // 2. the acceptance half-spans and radial reject bounds on the host,
+        //    with the routine grt_upload_grid uses (glibc arithmetic), so both
+        //    entry points accept and reject the same samples at cell edges
+        std::lock_guard<std::mutex> lock(g_stage_mutex);
+        const size_t nax = nr + nth + nph;
+        double* ha = g_stage_host;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ha, axes, nax * sizeof(double), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_fail(e);
+        const double *ra = ha, *ta = ha + nr, *pa = ha + nr + nth;
+        const bool sep = gm.separable != 0 && grt::axes::axes_stageable(ra, nr, ta, nth, pa, nph);
+        gm.separable = sep ? 1 : 0;
+        gm.r_reject_lo = 0.0;
+        gm.r_reject_hi = INFINITY;
+        if (sep) {
+            double* hh = ha + nax;
+            grt::axes::half_spans(ra, nr, 0, hh);
+            grt::axes::half_spans(ta, nth, 1, hh + nr);
+            grt::axes::half_spans(pa, nph, 2, hh + nr + nth);
+            grt::axes::radial_reject_bounds(ra, nr, &gm.r_reject_lo, &gm.r_reject_hi);
+            // returns once the pageable source is staged, so the buffer may be
+            // reused after the lock is released
+            e = cudaMemcpyAsync(axes + nax, hh, nax * sizeof(double), cudaMemcpyHostToDevice, stream);
+            if (e != cudaSuccess) return cuda_fail(e);
+        }
     }
     kp.a = p->spin;
     kp.M = p->mass;
@@ -328,6 +323,8 @@ extern "C" grt_status grt_trace_device_noalloc(const grt_params* p, const grt_de
         if (host.max_term_step > max_term_step) max_term_step = host.max_term_step;
         if (host.timed_out) {
             st.timed_out = 1;
+            st.steps_done = steps_done;
+            st.n_terminated = terminated;
             if (stats) *stats = st;
             set_err(err, err_len, "trace kernel hit its iteration limit");
             return GRT_ETIMEOUT;

@@ -2,11 +2,13 @@
 // built into lib/libgrt_selftest.so (test infrastructure; the product library
 // does not link it), with -fmad=false like the trace kernels.
 //   grt_selftest_division  div_by(a, b, RN(1/b)) and IEEE a / b on the same operands;
-//   grt_selftest_rhs       ks_rhs_rcp (and its box flag) and ks_rhs on the same states.
+//   grt_selftest_rhs       ks_rhs_rcp (and its box flag) and ks_rhs on the same states;
+//   grt_selftest_pow_quarter  the RK45 controller's pow_quarter on the device.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "grt_metric.cuh"
+#include "grt_pow_quarter.cuh"
 
 namespace {
 
@@ -32,6 +34,12 @@ __global__ void rhs_kernel(const double* st, size_t n, double spin, double M, do
         ieee[7 * i + c] = wv[c];
     }
     inside[i] = ok ? 1u : 0u;
+}
+
+__global__ void pow_quarter_kernel(const double* x, size_t n, double* y) {
+    const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    y[i] = grt::pow_quarter(x[i]);
 }
 
 template <int N>
@@ -97,6 +105,20 @@ int grt_selftest_rhs(const double* states, size_t n, double spin, double M, doub
     CK(cudaMemcpy(fast, df, 7 * n * 8, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(ieee, dw, 7 * n * 8, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(inside, din, n * 4, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+// y[i] = grt::pow_quarter(x[i]) evaluated on the device; host arrays of n.
+int grt_selftest_pow_quarter(const double* x, size_t n, double* y) {
+    if (n == 0) return 0;
+    Bufs<2> B;
+    double *dx, *dy;
+    CK(B.get(&dx, n));
+    CK(B.get(&dy, n));
+    CK(cudaMemcpy(dx, x, n * 8, cudaMemcpyHostToDevice));
+    pow_quarter_kernel<<<static_cast<unsigned>((n + 255) / 256), 256>>>(dx, n, dy);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(y, dy, n * 8, cudaMemcpyDeviceToHost));
     return 0;
 }
 

@@ -17,7 +17,7 @@
 #pragma once
 
 #include "grt_device.cuh"
-#include "grt_fourth_root.cuh"
+#include "grt_pow_quarter.cuh"
 
 namespace grt {
 namespace dev {
@@ -253,9 +253,9 @@ struct KStore {
     GRT_DEV double& at(int j, int c) const { return base[(j * 7 + c) * kTraceThreads]; }
 };
 
-// pow(1/err, 0.25) of the reference, correctly rounded (grt_fourth_root.cuh);
-// out of line to keep the step loop small.
-static __device__ __noinline__ double controller_root(double x) { return fourth_root_cr(x); }
+// pow(1/err, 0.25) of the reference as glibc's pow rounds it
+// (grt_pow_quarter.cuh); out of line to keep the step loop small.
+static __device__ __noinline__ double controller_root(double x) { return pow_quarter(x); }
 
 // One Fehlberg attempt (integrate_cart_ks.hpp:159-227), preceded by the
 // call's k1 = f(state) when need_k1 (integrate_cart_ks.hpp:274-275); returns 1

@@ -99,7 +99,8 @@ class ImageProducts(C.Structure):
 
 class LaunchConfig(C.Structure):
     _fields_ = [("threads_per_block", _I32), ("blocks_per_sm", _I32),
-                ("refill_threshold", _I32), ("photons_per_grab", _I32), ("split_legs", _I32)]
+                ("refill_threshold", _I32), ("photons_per_grab", _I32), ("split_legs", _I32),
+                ("pad", _I32), ("max_iterations", C.c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -66,10 +66,13 @@ def load(path: Path | None = None):
     L.grt_upload_grid_numpy_dir.argtypes = [vp, C.c_char_p]
     L.grt_upload_photons.argtypes = [vp, P(PhotonSoA), C.c_size_t]
     L.grt_init_image_photons.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint64]
+    L.grt_init_image_photons_random.argtypes = [vp, C.c_uint64, C.c_uint64]
     L.grt_run.argtypes = [vp, P(RunStats)]
     L.grt_download_photons.argtypes = [vp, P(PhotonSoA)]
     L.grt_photon_count.argtypes = [vp]
     L.grt_photon_count.restype = C.c_size_t
+    L.grt_geodesic_count.argtypes = [vp]
+    L.grt_geodesic_count.restype = C.c_uint64
     L.grt_get_image_products.argtypes = [vp, P(ImageProducts)]
     L.grt_write_image_products_npz.argtypes = [vp, C.c_char_p, C.c_char_p]
     L.grt_get_launch_config.argtypes = [vp, P(LaunchConfig)]
@@ -114,7 +117,8 @@ def load(path: Path | None = None):
                  "grt_init_image_batch", "grt_get_batch_image_products", "grt_write_batch_products_npz",
                  "grt_render_graph", "grt_trace_device_noalloc", "grt_measure_fma_peaks", "grt_params_validate", "grt_params_from_toml", "grt_create", "grt_set_params",
                  "grt_set_stream", "grt_synchronize", "grt_upload_grid", "grt_upload_grid_numpy_dir",
-                 "grt_upload_photons", "grt_init_image_photons", "grt_run", "grt_download_photons",
+                 "grt_upload_photons", "grt_init_image_photons", "grt_init_image_photons_random", "grt_run",
+                 "grt_download_photons",
                  "grt_get_image_products", "grt_write_image_products_npz", "grt_get_launch_config",
                  "grt_set_launch_config"):
         getattr(L, name).restype = C.c_int
@@ -268,6 +272,10 @@ class Context:
     def init_image_photons(self, nx, ny, id_offset=0):
         self._check(self.lib.grt_init_image_photons(self._h, nx, ny, id_offset))
 
+    def init_image_photons_random(self, n, id_offset=0):
+        """n rays at the reference's random screen positions (Philox streams)."""
+        self._check(self.lib.grt_init_image_photons_random(self._h, n, id_offset))
+
     def init_image_rows(self, nx, ny, row0, nrows, id_offset=0):
         """Pixel rows [row0, row0 + nrows) of the nx x ny screen (one image split across ranks)."""
         self._check(self.lib.grt_init_image_rows(self._h, nx, ny, row0, nrows, id_offset))
@@ -370,6 +378,11 @@ class Context:
     @property
     def n(self):
         return int(self.lib.grt_photon_count(self._h))
+
+    @property
+    def geodesics(self):
+        """Geodesics a run traces (fewer than n when frequency channels share them)."""
+        return int(self.lib.grt_geodesic_count(self._h))
 
     def download_photons(self, out: PhotonArrays | None = None) -> PhotonArrays:
         out = out or PhotonArrays(self.n)

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define GRT_ABI_VERSION 4
+#define GRT_ABI_VERSION 5
 
 typedef enum grt_status {
     GRT_OK = 0,
@@ -154,7 +154,7 @@ typedef struct grt_image_products {
     uint64_t* arrived_count;      /* [1] */
 } grt_image_products;
 
-/* Launch shape of the trace kernel: the library's default is {128, 4, 8, 32, 1};
+/* Launch shape of the trace kernel: the library's default is {128, 4, 8, 32, 1, 0, 0};
  * grt/autotune.py times the candidates on a workload and picks one. */
 typedef struct grt_launch_config {
     int32_t threads_per_block;    /* 128 (the trace kernels' block size) */
@@ -164,6 +164,12 @@ typedef struct grt_launch_config {
     int32_t split_legs;           /* image mode: 1 = the backward legs, the packet generation at first
                                      fluid contact and the rest as three launches (same results, smaller
                                      loop bodies); 0 = one launch for whole rays */
+    int32_t pad;
+    int64_t max_iterations;       /* per-warp loop iterations a trace launch may take before it stops,
+                                     writes every photon back at its last call boundary and the run
+                                     returns GRT_ETIMEOUT (stats.timed_out = 1); 0 = automatic (a bound
+                                     well above any launch that makes progress).  A later grt_run
+                                     continues the photons from where they were left. */
 } grt_launch_config;
 
 typedef struct grt_ctx grt_ctx;
@@ -235,6 +241,19 @@ grt_status grt_upload_photons(grt_ctx* ctx, const grt_photon_soa* soa, size_t n)
 grt_status grt_init_image_photons(grt_ctx* ctx, uint64_t nx, uint64_t ny, uint64_t id_offset);
 
 /*
+ * Initialise n image-plane photons on the device with the reference's random
+ * screen: replaces initialize_photons_image
+ * (src/radiative_transfer/initialize_photons.hpp:82-170) as it stands, whose
+ * screen position is (u, v) = (drand(-W/2, W/2), drand(-H/2, H/2)) from a
+ * random pool seeded 12345 + rank (:115-126).  Here each photon's two draws
+ * come from Philox4x32-10 keyed by (12345 + params.rank, photon id), so they
+ * do not depend on scheduling: u = -W/2 + W d1, v = -H/2 + H d2 with d in
+ * [0, 1), photon id = id_offset + i.  The rays are binned into the
+ * output.image_nx x image_ny image of grt_get_image_products, as there.
+ */
+grt_status grt_init_image_photons_random(grt_ctx* ctx, uint64_t n, uint64_t id_offset);
+
+/*
  * The pixel rows [row0, row0 + nrows) of the nx*ny screen of
  * grt_init_image_photons (same rays, same ids id_offset + iy*nx + ix): one
  * image split across GPUs, each rank tracing its rows; every rank's
@@ -270,6 +289,10 @@ grt_status grt_run(grt_ctx* ctx, grt_run_stats* stats);
 /* Copy the photon state back to host SoA (NULL fields are skipped). */
 grt_status grt_download_photons(grt_ctx* ctx, grt_photon_soa* soa);
 size_t grt_photon_count(const grt_ctx* ctx);
+/* Geodesics a run traces (no counterpart in the reference): the photon count,
+ * or, for a batch whose frequency channels share their geodesic
+ * (grt_set_channel_sharing, scattering off), one per channel group and pixel. */
+uint64_t grt_geodesic_count(const grt_ctx* ctx);
 
 /*
  * Host photon block (no counterpart in the reference, whose Photons are 20
@@ -500,10 +523,16 @@ typedef struct grt_device_grid {
  * library that each GPU loading the library holds until exit, shared by all
  * calls: serialise calls per device, because calls that overlap on the GPU
  * race on it.  Limits: nr + ntheta + nphi <= 8160 (larger grids are rejected
- * with GRT_EINVAL and a message), FP64 precision only.  The first call on a
- * device looks up the scratch address (cudaGetSymbolAddress) with that device
- * current; make it before any stream capture.  err receives a message on
- * failure (may be NULL).
+ * with GRT_EINVAL and a message), FP64 precision only.  Each call checks the
+ * grid's separability on the device (one pass over the coordinate arrays),
+ * then reads the axes back and derives the lookup's acceptance bounds on the
+ * host with the routine grt_upload_grid uses, so results equal the context
+ * entry point's bit for bit, cell edges included; the call waits for that
+ * read-back and for the trace on `stream` before it returns.  The first call
+ * on a device looks up the scratch address (cudaGetSymbolAddress) with that
+ * device current; make it before any stream capture.  err receives a message
+ * on failure (may be NULL).  When a launch runs out of iterations the call
+ * returns GRT_ETIMEOUT with stats filled as grt_run fills them.
  */
 grt_status grt_trace_device_noalloc(const grt_params* p, const grt_device_grid* grid,
                                     const grt_photon_soa* photons, uint64_t n, grt_run_stats* stats,

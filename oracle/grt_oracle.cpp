@@ -22,7 +22,7 @@
 #include <vector>
 
 #include "grt.h"
-#include "grt_fourth_root.cuh"  // the product's controller root, checked below against cr::fourth_root
+#include "grt_pow_quarter.cuh"  // the kernels' controller root, checked below against std::pow
 #include "grt_sincos.h"        // deterministic sin/cos shared with the kernels (scattering directions)
 #include "grt_user_physics.h"
 
@@ -30,91 +30,14 @@ namespace oracle {
 
 using real = double;
 
-// How the RK45 controller evaluates pow(1/err, 0.25):
-//   0 = correctly rounded fourth root (what the sm_100a kernels compute);
-//   1 = std::pow, i.e. glibc, exactly like the reference's host build.
+// How the RK45 controller evaluates pow(1/err, 0.25)
+// (src/geodesic_integrate/integrate_cart_ks.hpp:217):
+//   0 = std::pow, i.e. glibc, exactly like the reference's host build (default);
+//   1 = grt::pow_quarter, the kernels' restatement of glibc's pow compiled for
+//       the host (grt_pow_quarter.cuh), to show whole runs agree either way.
 int g_pow_mode = 0;
 
-// Correctly rounded x^(1/4), written independently of the kernel's version:
-// start from sqrt(sqrt(x)) and step while x lies beyond the fourth power of a
-// rounding midpoint, compared exactly with 32-bit limbs.
-namespace cr {
-using limbs = std::vector<uint64_t>;  // base 2^32, little endian
-limbs from_u64(uint64_t v) { return {v & 0xffffffffu, v >> 32}; }
-limbs mul(const limbs& a, const limbs& b) {
-    limbs r(a.size() + b.size() + 1, 0);
-    for (size_t i = 0; i < a.size(); ++i) {
-        uint64_t carry = 0;
-        for (size_t j = 0; j < b.size(); ++j) {
-            const uint64_t t = r[i + j] + a[i] * b[j] + carry;
-            r[i + j] = t & 0xffffffffu;
-            carry = t >> 32;
-        }
-        size_t k = i + b.size();
-        while (carry) {
-            const uint64_t t = r[k] + carry;
-            r[k] = t & 0xffffffffu;
-            carry = t >> 32;
-            ++k;
-        }
-    }
-    return r;
-}
-limbs shl(uint64_t v, int s) {  // v * 2^s
-    limbs r(static_cast<size_t>(s / 32 + 4), 0);
-    const int w = s / 32, b = s % 32;
-    const unsigned __int128 x = static_cast<unsigned __int128>(v) << b;
-    for (int q = 0; q < 3; ++q) r[w + q] = static_cast<uint64_t>(x >> (32 * q)) & 0xffffffffu;
-    return r;
-}
-int cmp(limbs a, limbs b) {
-    while (a.size() < b.size()) a.push_back(0);
-    while (b.size() < a.size()) b.push_back(0);
-    for (size_t k = a.size(); k-- > 0;)
-        if (a[k] != b[k]) return a[k] > b[k] ? 1 : -1;
-    return 0;
-}
-void split(double v, uint64_t& m, int& e) {
-    int ex;
-    const double f = std::frexp(v, &ex);  // v = f 2^ex, f in [0.5, 1)
-    m = static_cast<uint64_t>(std::ldexp(f, 53));
-    e = ex - 53;
-    while (m && !(m & 1)) { m >>= 1; ++e; }
-}
-// sign of A^4 2^(4 ea) - X 2^ex
-int cmp_mid4(uint64_t A, int ea, uint64_t X, int ex) {
-    const limbs a = from_u64(A);
-    const limbs p = mul(mul(a, a), mul(a, a));
-    const int s = ex - 4 * ea;
-    if (s >= 0) return cmp(p, shl(X, s));
-    return cmp(mul(p, shl(1, -s)), from_u64(X));
-}
-double fourth_root(double x) {
-    if (!(x > 0.0) || !std::isfinite(x)) return std::sqrt(std::sqrt(x));
-    double y = std::sqrt(std::sqrt(x));
-    uint64_t X;
-    int ex;
-    split(x, X, ex);
-    for (int it = 0; it < 4; ++it) {
-        const double up = std::nextafter(y, INFINITY), dn = std::nextafter(y, 0.0);
-        // midpoints as odd integers times powers of two
-        uint64_t Mu; int eu; split(y + 0.0, Mu, eu);
-        const double hi_gap = up - y, lo_gap = y - dn;
-        int eg; uint64_t g;
-        split(hi_gap, g, eg);  // gap is a power of two: g == 1
-        // y = Mu 2^eu; mid_up = y + gap/2 = (Mu 2^(eu-eg+1) + 1) 2^(eg-1)
-        const uint64_t Aup = (Mu << (eu - eg + 1)) + 1;
-        if (cmp_mid4(Aup, eg - 1, X, ex) < 0) { y = up; continue; }
-        split(lo_gap, g, eg);
-        const uint64_t Adn = (Mu << (eu - eg + 1)) - 1;
-        if (cmp_mid4(Adn, eg - 1, X, ex) > 0) { y = dn; continue; }
-        break;
-    }
-    return y;
-}
-}  // namespace cr
-
-real controller_root(real x) { return g_pow_mode == 1 ? std::pow(x, real(0.25)) : cr::fourth_root(x); }
+real controller_root(real x) { return g_pow_mode == 1 ? grt::pow_quarter(x) : std::pow(x, real(0.25)); }
 using grt::FluidCellCGS;
 
 constexpr real PI = 3.14159265358979323846;  // src/utils.hpp:16
@@ -1343,6 +1266,50 @@ int oracle_init_disk_photons(const grt_params* p, size_t nr, size_t nth, size_t 
 
 // Deterministic pixel-grid variant of initialize_photons_image
 // (src/radiative_transfer/initialize_photons.hpp:82-170).
+// initialize_photons_image (src/radiative_transfer/initialize_photons.hpp:
+// 82-170) with its random screen (:115-126): (u, v) = drand(-W/2, W/2),
+// drand(-H/2, H/2), drand(lo, hi) = lo + (hi - lo) d, the pool seeded
+// 12345 + rank -- here Philox keyed by (12345 + rank, photon id, domain
+// 0xFFFFFFFE), the kernels' streams, in place of Kokkos's XorShift pool.
+int oracle_init_image_photons_random(const grt_params* p, uint64_t n, uint64_t id_offset, grt_photon_soa* out) {
+    const real D = p->camera_distance;
+    const real cx = D * std::sin(p->camera_theta) * std::cos(p->camera_phi);
+    const real cy = D * std::sin(p->camera_theta) * std::sin(p->camera_phi);
+    const real cz = D * std::cos(p->camera_theta);
+    const real th_hat[3] = {std::cos(p->camera_theta) * std::cos(p->camera_phi),
+                            std::cos(p->camera_theta) * std::sin(p->camera_phi), -std::sin(p->camera_theta)};
+    const real ph_hat[3] = {-std::sin(p->camera_phi), std::cos(p->camera_phi), 0.0};
+    const real W = p->camera_width, H = p->camera_height;
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t id = id_offset + i;
+        Philox rng(12345ull + static_cast<uint64_t>(static_cast<int64_t>(p->rank)), id, 0xFFFFFFFEu);
+        const real u = -W / 2 + (W / 2 - (-W / 2)) * rng.drand();
+        const real v = -H / 2 + (H / 2 - (-H / 2)) * rng.drand();
+        out->id[i] = id;
+        out->frequency[i] = 0.0;
+        out->emission_frame_energy[i] = 1.0;
+        const real x = cx + u * th_hat[0] + v * ph_hat[0];
+        const real y = cy + u * th_hat[1] + v * ph_hat[1];
+        const real z = cz + u * th_hat[2] + v * ph_hat[2];
+        real kx = -cx, ky = -cy, kz = -cz;
+        const real kn = std::sqrt(kx * kx + ky * ky + kz * kz);
+        kx /= kn; ky /= kn; kz /= kn;
+        out->x0[i] = 0.0; out->x1[i] = x; out->x2[i] = y; out->x3[i] = z;
+        const real X[4] = {0.0, x, y, z};
+        const real K[3] = {kx, ky, kz};
+        real pc[4] = {0.0, 0.0, 0.0, 0.0};
+        null_covariant_momentum(X, K, p->spin, p->mass, pc);
+        out->k0[i] = pc[0]; out->k1[i] = pc[1]; out->k2[i] = pc[2]; out->k3[i] = pc[3];
+        out->I[i] = out->Q[i] = out->U[i] = out->V[i] = 0.0;
+        out->dlambda[i] = p->initial_step * D;
+        out->terminate[i] = 0;
+        out->phase[i] = GRT_PHASE_IMAGE_BACKWARD;
+        out->theta_disp[i] = u;
+        out->phi_disp[i] = v;
+    }
+    return 0;
+}
+
 int oracle_init_image_photons(const grt_params* p, uint64_t nx, uint64_t ny, uint64_t id_offset,
                               grt_photon_soa* out) {
     const real D = p->camera_distance;
@@ -1544,15 +1511,14 @@ void oracle_set_pow_mode(int mode) { g_pow_mode = mode; }
 void oracle_det_sincos(const double* x, uint64_t n, double* s, double* c) {
     for (uint64_t i = 0; i < n; ++i) grt::det_sincos(x[i], s + i, c + i);
 }
-double oracle_fourth_root(double x) { return cr::fourth_root(x); }
-// Element-wise: out_oracle[i] = the oracle's arbitrary-precision root,
-// out_product[i] = the product's fourth_root_cr (rounding test + 256-bit
-// fallback) compiled for the host; the two must agree bit for bit.
-void oracle_fourth_root_pair(const double* x, uint64_t n, double* out_oracle, double* out_product) {
+// Element-wise: out_libm[i] = std::pow(x[i], 0.25) from this host's libm,
+// out_product[i] = the kernels' grt::pow_quarter compiled for the host; the two
+// must agree bit for bit.
+void oracle_pow_quarter_pair(const double* x, uint64_t n, double* out_libm, double* out_product) {
 #pragma omp parallel for schedule(static)
     for (long long i = 0; i < static_cast<long long>(n); ++i) {
-        out_oracle[i] = cr::fourth_root(x[i]);
-        out_product[i] = grt::fourth_root_cr(x[i]);
+        out_libm[i] = std::pow(x[i], 0.25);
+        out_product[i] = grt::pow_quarter(x[i]);
     }
 }
 // Algorithmic op counts (add+sub, mul, div, sqrt, pow) of one RHS, one RK4
@@ -1595,9 +1561,7 @@ void oracle_op_counts(const grt_params* p, const double X[4], const double P[4],
     take(rk45_ops);
     st.rhs(sd2, kd);
     double dld = dl;
-    g_pow_mode = 1;
     st.rk45(sd2, &dld, kd);
-    g_pow_mode = 0;
     checks[2] = std::fabs(dld - dln.v);
     for (int q = 0; q < 8; ++q) checks[2] = std::fmax(checks[2], std::fabs(sd2[q] - s2[q].v));
 }

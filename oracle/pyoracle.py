@@ -48,6 +48,7 @@ class Oracle:
         L.oracle_run.argtypes = [P, C.c_size_t, C.c_size_t, C.c_size_t] + [_DP] * 9 + [
             C.POINTER(PhotonSoA), C.c_size_t, C.POINTER(RunStats)]
         L.oracle_init_image_photons.argtypes = [P, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(PhotonSoA)]
+        L.oracle_init_image_photons_random.argtypes = [P, C.c_uint64, C.c_uint64, C.POINTER(PhotonSoA)]
         L.oracle_image_products.argtypes = [P, C.POINTER(PhotonSoA), C.c_size_t, C.POINTER(ImageProducts)]
         L.oracle_hamiltonian_rhs.argtypes = [_DP, _DP, C.c_double, C.c_double, _DP]
         L.oracle_compute_r.argtypes = [C.c_double] * 4
@@ -67,10 +68,8 @@ class Oracle:
         L.oracle_philox_drand.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_int]
         L.oracle_philox_drand.restype = C.c_double
         L.oracle_set_pow_mode.argtypes = [C.c_int]
-        L.oracle_fourth_root.argtypes = [C.c_double]
-        L.oracle_fourth_root.restype = C.c_double
-        L.oracle_fourth_root_pair.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
-        L.oracle_fourth_root_pair.restype = None
+        L.oracle_pow_quarter_pair.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.oracle_pow_quarter_pair.restype = None
         L.oracle_observation_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint64]
         L.oracle_observation_bin.restype = C.c_uint64
         L.oracle_init_disk_photons.argtypes = ([P] + [C.c_size_t] * 3 + [_DP] * 7 +
@@ -83,15 +82,22 @@ class Oracle:
                                              [C.POINTER(PhotonSoA), C.c_size_t, _DP, _DP, _DP])
 
     def set_pow_mode(self, mode):
-        """'cr': correctly rounded controller root (kernel semantics);
-        'libm': std::pow like the reference's host build."""
-        self.lib.oracle_set_pow_mode({"cr": 0, "libm": 1}[mode])
+        """The RK45 controller's pow(1/err, 0.25): 'libm' (default) calls
+        std::pow like the reference's host build; 'restated' calls the
+        kernels' grt::pow_quarter compiled for the host."""
+        self.lib.oracle_set_pow_mode({"libm": 0, "restated": 1}[mode])
 
     # ---- whole-path entry points ----
     def init_image_photons(self, p: Params, nx, ny, id_offset=0) -> PhotonArrays:
         ph = PhotonArrays(nx * ny)
         soa = ph.soa()
         self.lib.oracle_init_image_photons(C.byref(p), nx, ny, id_offset, C.byref(soa))
+        return ph
+
+    def init_image_photons_random(self, p: Params, n, id_offset=0) -> PhotonArrays:
+        ph = PhotonArrays(n)
+        soa = ph.soa()
+        self.lib.oracle_init_image_photons_random(C.byref(p), n, id_offset, C.byref(soa))
         return ph
 
     def init_disk_photons(self, p: Params, grid: dict, id_offset=0) -> PhotonArrays:
@@ -183,6 +189,7 @@ class Reference:
         L.ref_last_error.restype = C.c_char_p
         L.ref_params_from_toml.argtypes = [C.c_char_p, C.POINTER(Params)]
         L.ref_init_image_photons.argtypes = [C.c_char_p, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(PhotonSoA)]
+        L.ref_init_image_photons_random.argtypes = [C.c_char_p, C.c_uint64, C.c_uint64, C.POINTER(PhotonSoA)]
         L.ref_run_photons.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(PhotonSoA), C.c_uint64,
                                       C.POINTER(ImageProducts), _DP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.ref_init_disk_photons.argtypes = [C.c_char_p, C.c_char_p, C.c_uint64, C.POINTER(PhotonSoA),
@@ -197,6 +204,17 @@ class Reference:
     @staticmethod
     def available():
         return REF_SO.exists()
+
+    @staticmethod
+    def root():
+        """The reference project's root directory oracle/_ref was built from,
+        when that tree is present on this machine (else None)."""
+        f = REF_SO.parent / "reference_root.txt"
+        try:
+            root = Path(f.read_text().strip())
+        except OSError:
+            return None
+        return root if root.is_dir() else None
 
     def error(self):
         return self.lib.ref_last_error().decode()
@@ -219,6 +237,14 @@ class Reference:
         ph = PhotonArrays(nx * ny)
         soa = ph.soa()
         if self.lib.ref_init_image_photons(str(toml).encode(), nx, ny, id_offset, C.byref(soa)) != 0:
+            raise ValueError(self.error())
+        return ph
+
+    def init_image_photons_random(self, toml, n, id_offset=0) -> PhotonArrays:
+        """The reference's own initialize_photons_image, random screen and all."""
+        ph = PhotonArrays(n)
+        soa = ph.soa()
+        if self.lib.ref_init_image_photons_random(str(toml).encode(), n, id_offset, C.byref(soa)) != 0:
             raise ValueError(self.error())
         return ph
 

@@ -226,6 +226,26 @@ int ref_init_image_photons(const char* toml_path, std::uint64_t nx, std::uint64_
     return 0;
 }
 
+// The reference's own initialize_photons_image
+// (src/radiative_transfer/initialize_photons.hpp:82-170) with its random
+// screen draw, on rank 0 of 1, through the shim's random pool (its own
+// XorShift streams, not Kokkos's): n photons with ids id_offset + i.
+int ref_init_image_photons_random(const char* toml_path, std::uint64_t n, std::uint64_t id_offset,
+                                  grt_photon_soa* out) {
+    Loaded cfg;
+    if (!load_config(toml_path, cfg)) return 1;
+    try {
+        Photons photons(static_cast<int>(n), "photons_");
+        initialize_photons_image(static_cast<int>(n), camera_distance, camera_theta, camera_phi, 0, 1, id_offset,
+                                 photons);
+        to_soa(photons, out);
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 2;
+    }
+}
+
 // Run the reference's integrate_geodesics on n caller-provided photons (in
 // place), with the grid from the config's input.numpy_dir (numpy_dir_override
 // replaces it when non-NULL) and output archives under output_dir.  When

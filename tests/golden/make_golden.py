@@ -3,7 +3,9 @@
 Run in a container where the reference tree is available (it is not on the
 GPU box; the fixtures are committed instead):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference project root>
+
+(or GRT_REFERENCE_ROOT=<reference project root> in the environment)
 
 Produces:
   torus_reference.npz  -- arrays written by the reference's own
@@ -27,6 +29,7 @@ from __future__ import annotations
 
 import argparse
 import importlib.util
+import os
 import json
 import sys
 import tempfile
@@ -70,8 +73,10 @@ def npy_loader_grid():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("GRT_REFERENCE_ROOT"))
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("--reference (or GRT_REFERENCE_ROOT) must name the reference project's root")
     ref_src = Path(args.reference) / "src"
 
     # 1. torus arrays from the reference script

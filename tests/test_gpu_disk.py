@@ -83,7 +83,10 @@ def test_disk_escape_distribution_matches_reference(gpu, reference):
         assert pv > 0.01, (k, pv)
 
 
-def test_disk_workload_1e7_packets(gpu):
+@pytest.fixture(scope="module")
+def c5_run(gpu):
+    """The C5 workload on the GPU: ~1e7 packets from the 128x64x64 torus
+    (a = 0.9), RK45, elastic Thomson scattering, absorption and emission."""
     w = workloads.C5
     p = w.params()
     grid = w.torus()
@@ -92,7 +95,6 @@ def test_disk_workload_1e7_packets(gpu):
         ctx.upload_grid(grid)
         t0 = time.perf_counter()
         n = ctx.init_disk_photons()
-        assert 0.9e7 <= n <= 1.1e7
         q = p.copy()
         q.nphotons = n
         ctx.set_params(q)
@@ -101,9 +103,74 @@ def test_disk_workload_1e7_packets(gpu):
         ph = ctx.download_photons()
     finally:
         ctx.close()
+    return p, grid, n, st, dt, ph
+
+
+def test_disk_workload_1e7_packets(c5_run):
+    p, _, n, st, dt, ph = c5_run
+    assert 0.9e7 <= n <= 1.1e7
     assert st["timed_out"] == 0 and st["n_terminated"] == n
     esc, s = escape_samples(ph, p)
     assert 0.5 < esc.mean() <= 1.0
     assert np.all(np.isfinite(s["E"])) and np.all(s["E"] > 0)
     print(f"c5: {n} packets, {st['accepted_steps']} accepted steps, trace {st['trace_ms']:.1f} ms, "
           f"wall {dt:.2f} s, escape fraction {esc.mean():.4f}")
+
+
+def weighted_chi2(w1, v1, w2, v2):
+    """Two weighted histograms (bin sums w, bin sums of squared weights v),
+    each normalised to unit total: X^2 = sum (w1/W1 - w2/W2)^2 /
+    (v1/W1^2 + v2/W2^2) over bins with entries, ~ chi^2(k - 1)."""
+    W1, W2 = w1.sum(), w2.sum()
+    var = v1 / W1 ** 2 + v2 / W2 ** 2
+    m = var > 0
+    x2 = float(np.sum((w1[m] / W1 - w2[m] / W2) ** 2 / var[m]))
+    return x2, int(m.sum()) - 1
+
+
+def test_c5_escape_histograms_match_reference(c5_run, reference, tmp_path):
+    """The escape histograms of the C5 workload -- 64 bins of I-weighted
+    escape energy -p_t and 64 x 64 bins of escape direction (cos theta, phi)
+    -- against the reference's own code on the same 128x64x64 grid.  The
+    reference's emission (its cell offsets and initialiser, through the shim's
+    random pool) gives its ~1e7 packets; every 64th of them (about 155,000
+    packets, ten to twenty seconds of CPU transport) is traced by the
+    reference's step loop.  Its random streams differ from the product's, so
+    the comparison is statistical: chi^2 on the histograms, KS on the
+    samples, the escape fraction within binomial noise."""
+    p, grid, n, _, _, mine = c5_run
+    torus.write_numpy_dir(grid, tmp_path / "np")
+    toml = config.write_toml(p, tmp_path / "c.toml", tmp_path / "np", tmp_path / "out")
+    full = reference.init_disk_photons(toml)
+    assert abs(full.n - n) <= 0.01 * n  # the same emission counts, up to the draws
+    ref = abi.PhotonArrays.from_dict({f: np.ascontiguousarray(getattr(full, f)[::64]) for f in abi.PHOTON_FIELDS})
+    del full
+    q = p.copy()
+    q.nphotons = ref.n
+    reference.run(toml, ref, q)
+    em, sm = escape_samples(mine, p)
+    er, sr = escape_samples(ref, p)
+    f1, f2 = em.mean(), er.mean()
+    sd = np.sqrt(f1 * (1 - f1) / mine.n + f2 * (1 - f2) / ref.n)
+    assert abs(f1 - f2) <= 4 * sd, (f1, f2)
+    # 64 energy bins, equally populated in the product's (large) sample
+    edges = np.quantile(sm["E"], np.linspace(0.0, 1.0, 65))
+    edges[0], edges[-1] = -np.inf, np.inf
+    wm, wr = mine.I[em], ref.I[er]
+    h = [np.histogram(s_["E"], bins=edges, weights=w_)[0] for s_, w_ in ((sm, wm), (sr, wr))]
+    v = [np.histogram(s_["E"], bins=edges, weights=w_ * w_)[0] for s_, w_ in ((sm, wm), (sr, wr))]
+    x2, dof = weighted_chi2(h[0], v[0], h[1], v[1])
+    p_energy = scipy_stats.chi2.sf(x2, dof)
+    assert p_energy > 0.01, (x2, dof)
+    # 64 x 64 direction bins (cos theta, phi), counts
+    bins = [np.linspace(-1.0, 1.0, 65), np.linspace(-np.pi, np.pi, 65)]
+    cm = np.histogram2d(sm["cos"], sm["phi"], bins=bins)[0].ravel()
+    cr = np.histogram2d(sr["cos"], sr["phi"], bins=bins)[0].ravel()
+    keep = (cm + cr) > 0
+    chi2, p_dir, dof_dir, _ = scipy_stats.chi2_contingency(np.vstack([cm[keep], cr[keep]]))
+    assert p_dir > 0.01, (chi2, dof_dir)
+    for k in ("E", "cos", "phi"):
+        pv = scipy_stats.ks_2samp(sm[k], sr[k]).pvalue
+        assert pv > 0.01, (k, pv)
+    print(f"c5 histograms: product {mine.n} packets, reference {ref.n}; escape fraction {f1:.4f} vs {f2:.4f}; "
+          f"energy chi2 p = {p_energy:.3g}, direction chi2 p = {p_dir:.3g}")

@@ -12,7 +12,10 @@ the trace kernels):
 * ks_rhs_rcp against ks_rhs (IEEE divisions), all seven components bit for
   bit, on random photon states from the horizon to 2000 M, with exactly zero
   coordinates, for several spins; states outside the box (coordinates of
-  magnitude below 2^-20 or above 2^20) must be reported outside."""
+  magnitude below 2^-20 or above 2^20) must be reported outside;
+* the RK45 controller's pow_quarter on the device against this host's glibc
+  pow(x, 0.25), bit for bit, on tie-near inputs (tests/golden/pow_quarter_hard.npz)
+  and on random inputs over the controller's range and over all doubles."""
 
 import ctypes as C
 from pathlib import Path
@@ -34,6 +37,7 @@ def selftest(gpu):
     L = C.CDLL(str(LIB))
     L.grt_selftest_division.argtypes = [_DP, _DP, C.c_size_t, _DP, _DP]
     L.grt_selftest_rhs.argtypes = [_DP, C.c_size_t, C.c_double, C.c_double, _DP, _DP, _UP]
+    L.grt_selftest_pow_quarter.argtypes = [_DP, C.c_size_t, _DP]
     return L
 
 
@@ -146,3 +150,20 @@ def test_states_outside_the_box_are_reported(selftest):
     s[5, 0] = 2.0 ** -20
     _, _, inside = rhs(selftest, s, 0.9)
     assert inside.tolist() == [False, False, False, False, True, True]
+
+
+def test_device_pow_quarter_is_glibc_pow(selftest, oracle):
+    from conftest import GOLDEN
+    g = np.load(GOLDEN / "pow_quarter_hard.npz")
+    rng = np.random.default_rng(17)
+    xs = [g["x_controller"], g["x_wide"], np.exp(rng.uniform(np.log(1.5e-8), np.log(2e4), 4_000_000)),
+          rng.integers(0, 0x7FF0000000000000, 1_000_000, dtype=np.uint64).view(np.float64),
+          np.array([0.0, -0.0, np.inf, -np.inf, 5e-324, 2.0 ** -1022, 1.0, 1.0 + 2.0 ** -52, 1.0 - 2.0 ** -53])]
+    x = np.ascontiguousarray(np.concatenate(xs))
+    y = np.empty_like(x)
+    assert selftest.grt_selftest_pow_quarter(dp(x), x.size, dp(y)) == 0
+    want, host = np.empty_like(x), np.empty_like(x)  # std::pow (glibc) and the host build
+    oracle.lib.oracle_pow_quarter_pair(x.ctypes.data, C.c_uint64(x.size), want.ctypes.data, host.ctypes.data)
+    assert_bitwise(y, want)
+    assert_bitwise(host, want)
+    assert np.array_equal(y[: g["x_controller"].size], g["pow_controller"])

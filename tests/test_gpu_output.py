@@ -1,16 +1,14 @@
 """Output-step archives (write_output_step, src/output/write_output.hpp:90-103)
 through grt_run_with_output, the reference's whole step loop with its output.
 
-* Fixed-step RK4 trajectories are bit-identical to the reference's, so every
-  output-step archive must equal, byte for byte, the archive the reference's
-  own integrate_geodesics writes (oracle/_ref) for the same config -- the same
-  files (same output steps, same stop), members, dtypes, strides and values;
-  the image-products archive agrees to round-off (device atomics add in
-  another order).
-* RK45 (the controller's fourth root is correctly rounded here, libm's pow in
-  the reference): every archive has the reference's layout, the last one holds
-  the final photon state, and an intermediate one equals the state after that
-  many steps of a separate run."""
+Fixed-step RK4 and adaptive RK45 trajectories are bit-identical to the
+reference's (the RK45 controller's pow rounds as glibc's does), so every
+output-step archive must equal, byte for byte, the archive the reference's own
+integrate_geodesics writes (oracle/_ref) for the same config -- the same files
+(same output steps, same stop), members, dtypes, strides and values; the
+image-products archive agrees to round-off (device atomics add in another
+order).  An RK45 archive also equals the state after that many steps of a
+separate run."""
 
 import io
 import zipfile
@@ -70,9 +68,18 @@ def step_files(d):
     return sorted((f.name for f in d.iterdir() if "_step_" in f.name), key=step_of)
 
 
-@pytest.mark.parametrize("variables,stride", [("all", 3), ("id,frequency,x0,x1,x2,x3,k0,k1,k2,k3,I,Q,U,V,phase", 1)])
-def test_rk4_archives_are_the_references_bytes(gpu, reference, tmp_path, variables, stride):
-    w = mini(workloads.C1, 16, (24, 16, 16), termination_percent=0.9, output_interval=37)
+ARCHIVE_CASES = [
+    ("rk4", "all", 3), ("rk4", "id,frequency,x0,x1,x2,x3,k0,k1,k2,k3,I,Q,U,V,phase", 1),
+    ("rk45", "all", 2), ("rk45", "x0,x1,x2,x3,k0,k1,k2,k3,dlambda,I,phase,terminate", 1),
+]
+
+
+@pytest.mark.parametrize("form,variables,stride", ARCHIVE_CASES)
+def test_archives_are_the_references_bytes(gpu, reference, tmp_path, form, variables, stride):
+    if form == "rk4":
+        w = mini(workloads.C1, 16, (24, 16, 16), termination_percent=0.9, output_interval=37)
+    else:
+        w = mini(workloads.C2, 16, (32, 16, 16), termination_percent=0.9, output_interval=5)
     p = w.params()
     ref_dir = reference_archives(reference, p, w, tmp_path, variables, stride)
     ours = tmp_path / "ours"

@@ -53,30 +53,120 @@ def _to_host(t, n):
     return out
 
 
-@pytest.mark.parametrize("w", [mini(workloads.C2, 24, (32, 16, 16)), mini(workloads.C1, 12, (24, 16, 16))],
-                         ids=["rk45", "rk4"])
-def test_noalloc_matches_context_entry_point_twice(gpu, oracle, w):
-    torch = pytest.importorskip("torch")
-    p = w.params()
-    grid = w.torus()
-    init = oracle.init_image_photons(p, w.pixels, w.pixels)
-    want, _, wst = run_gpu(gpu, p, grid, photons=init)
-
+def _device_grid(torch, grid):
     dgrid = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in grid.items()}
     G = abi.DeviceGrid()
     G.nr, G.ntheta, G.nphi = grid["r.npy"].shape
     for field, key in (("r", "r.npy"), ("theta", "theta.npy"), ("phi", "phi.npy"), ("rho", "rho.npy"),
                        ("temperature", "Tgas.npy"), ("vel4", "vel.npy"), ("mag4", "mag.npy")):
         setattr(G, field, dgrid[key].data_ptr())
+    return dgrid, G
+
+
+def _twice_against_context(gpu, torch, p, grid, init, exact=False):
+    """Trace init through the context entry point once and through the
+    allocation-free one twice in a row; both allocation-free results must
+    match the context's (bit for bit when exact), with the same counts."""
+    want, _, wst = run_gpu(gpu, p, grid, photons=init)
+    dgrid, G = _device_grid(torch, grid)
     for _ in range(2):
         tensors, soa = _device_soa(torch, init)
         torch.cuda.synchronize()
         st = gpu.trace_device_noalloc(p, G, soa, init.n)
         torch.cuda.synchronize()
         got = _to_host(tensors, init.n)
-        assert_photons_match(got, want)
+        d = assert_photons_match(got, want)
+        if exact:
+            assert all(v == 0 for v in d.values()), d
         for key in ("accepted_steps", "rejected_attempts", "photon_calls", "n_terminated", "steps_done"):
             assert st[key] == wst[key], key
+    return want
+
+
+@pytest.mark.parametrize("w", [mini(workloads.C2, 24, (32, 16, 16)), mini(workloads.C1, 12, (24, 16, 16))],
+                         ids=["rk45", "rk4"])
+def test_noalloc_matches_context_entry_point_twice(gpu, oracle, w):
+    torch = pytest.importorskip("torch")
+    p = w.params()
+    _twice_against_context(gpu, torch, p, w.torus(), oracle.init_image_photons(p, w.pixels, w.pixels))
+
+
+def test_noalloc_non_separable_grid(gpu, oracle):
+    """Coordinates perturbed cell by cell, so the grid is not an outer product
+    of axes: both entry points take the reference's general three-pass lookup
+    on the raw coordinate arrays."""
+    torch = pytest.importorskip("torch")
+    w = mini(workloads.C2, 20, (32, 16, 16))
+    p = w.params()
+    grid = dict(w.torus())
+    rng = np.random.default_rng(8)
+    grid["r.npy"] = grid["r.npy"] * (1.0 + 1e-4 * rng.standard_normal(grid["r.npy"].shape))
+    grid["theta.npy"] = grid["theta.npy"] + 1e-5 * rng.standard_normal(grid["theta.npy"].shape)
+    want = _twice_against_context(gpu, torch, p, grid, oracle.init_image_photons(p, w.pixels, w.pixels), exact=True)
+    assert (want.phase == 3).sum() > 20  # rays arrived through the fluid
+
+
+def test_noalloc_disk_mode_with_scattering(gpu):
+    """Disk-mode packets from every cell, RK45, Thomson scattering on (Philox
+    draws keyed by packet id and step): photon for photon the same as the
+    context entry point."""
+    torch = pytest.importorskip("torch")
+    wd = workloads.DiskWorkload("disk_small", (32, 16, 16), 0.9, 6.0, max_steps=4000)
+    p = wd.params()
+    grid = wd.torus()
+    ctx = gpu.Context(p)
+    try:
+        ctx.upload_grid(grid)
+        n = ctx.init_disk_photons()
+        init = ctx.download_photons()
+    finally:
+        ctx.close()
+    assert n > 500
+    p.nphotons = n
+    want = _twice_against_context(gpu, torch, p, grid, init, exact=True)
+    assert (want.I != init.I).any()
+
+
+def test_noalloc_samples_at_radial_cell_edges(gpu):
+    """Photons placed so that their first fluid sample lands within a few ulp
+    of a radial acceptance boundary, log(r / r_i) = +-0.500001 * (largest log
+    spacing next to r_i): both entry points derive that bound with the same
+    host routine, so they accept and reject exactly the same samples."""
+    torch = pytest.importorskip("torch")
+    w = mini(workloads.C1, 8, (24, 16, 16), max_steps=2)
+    p = w.params()
+    grid = w.torus()
+    ra = grid["r.npy"][:, 0, 0]
+    nr = len(ra)
+    # interior edges (where the nearest cell changes) and the grid's inner
+    # and outer edges (where samples start to be rejected)
+    edges = []
+    for i in range(2, nr - 2, 3):
+        h = 0.500001 * max(abs(np.log(ra[i] / ra[i - 1])), abs(np.log(ra[i + 1] / ra[i])))
+        edges += [ra[i] * np.exp(h), ra[i] * np.exp(-h)]
+    edges += [ra[0] * np.exp(-0.500001 * abs(np.log(ra[0] / ra[1]))),
+              ra[nr - 1] * np.exp(0.500001 * abs(np.log(ra[nr - 1] / ra[nr - 2])))]
+    rows = [edge * (1.0 + k * 2.0 ** -52) for edge in edges for k in range(-24, 25)]
+    r = np.array(rows)
+    n = r.size
+    ph = abi.PhotonArrays(n)
+    ph.id[:] = np.arange(n, dtype=np.uint64)
+    # equatorial plane (theta = pi/2 is inside the torus), phi = 0:
+    # x^2 + y^2 = r^2 + a^2 for a Kerr-Schild radius r
+    ph.x1[:] = np.sqrt(r * r + p.spin * p.spin)
+    # a tiny momentum moves the photon by ~1e-14 M per unit of affine
+    # parameter, so the sample after a step of 1 stays within a few ulp of
+    # the start, while the transfer path of the step (|dlambda| = 1) is not small
+    ph.k0[:] = -1e-14
+    ph.k3[:] = 1e-16
+    ph.dlambda[:] = 1.0
+    ph.frequency[:] = 2.3e11
+    ph.emission_frame_energy[:] = 1.0
+    ph.I[:] = 1.0
+    ph.phase[:] = 2  # ImageForward: every step samples the fluid and applies transfer
+    want = _twice_against_context(gpu, torch, p, grid, ph, exact=True)
+    changed = want.I != 1.0
+    assert 0 < changed.sum() < n  # some samples accepted, some rejected at the edges
 
 
 def test_noalloc_rejects_oversized_grid(gpu):
