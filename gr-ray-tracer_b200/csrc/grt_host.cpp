@@ -1,16 +1,18 @@
-// Host-side formats of the hot path's boundary: the reference's flat TOML
-// config, its NumPy .npy grid inputs and its uncompressed .npz output archives.
+// Host-side formats of the hot path's boundary: the reference's NumPy .npy
+// grid inputs and its uncompressed .npz output archives, plus the defaults
+// and validity checks of grt_params.
 //
-//   grt_params_default / grt_params_from_toml / grt_params_validate mirror
-//     toml_config::parse_flat_toml + load_and_apply_toml_config
-//     (src/input/toml_config.hpp:40-77, 129-278) with defaults from
-//     src/utils.cpp:4-37, src/simulation_options.hpp:13-32 and
-//     src/radiative_transfer/photon_generation.hpp:18-50;
+//   grt_params_default fills the reference's compiled-in defaults
+//     (src/utils.cpp:4-37, src/simulation_options.hpp:13-32,
+//     src/radiative_transfer/photon_generation.hpp:18-50);
+//   grt_params_validate checks what the kernels need of a grt_params;
 //   npy_load_f64 reads what load_numpy_field_bundle accepts
 //     (src/input/load_python_arrays.hpp:115-193: '<f8'/'=f8', C order);
 //   NpzOut writes the byte layout of cnpy::NpzWriter (src/cnpy.h:146-300):
 //     NPY 1.0 members, 16-byte padded headers, STORED ZIP with zero timestamps,
 //     so archives are byte-for-byte the ones the reference writes.
+// The reference's TOML config is read by the reference's own loader; its
+// parsed structs reach the ABI through include/grt_reference_adapter.hpp.
 #include "grt_host.h"
 
 #include <algorithm>
@@ -37,10 +39,6 @@ void set_err(char* err, size_t len, const std::string& msg) {
     }
 }
 
-void set_str(char* dst, size_t len, const std::string& s) {
-    if (dst && len > 0) std::snprintf(dst, len, "%s", s.c_str());
-}
-
 std::string strip(const std::string& s) {
     const auto b = s.find_first_not_of(" \t\r\n");
     if (b == std::string::npos) return "";
@@ -48,120 +46,14 @@ std::string strip(const std::string& s) {
     return s.substr(b, e - b + 1);
 }
 
-using Raw = std::map<std::string, std::string>;
+// One condition of grt_params_validate and what it says when it fails.
+struct Rule {
+    bool ok;
+    const char* message;
+};
 
-// toml_config.hpp:40-77
-Raw parse_flat(const std::string& path) {
-    std::ifstream in(path);
-    if (!in) throw std::runtime_error("Failed to open config file: " + path);
-    Raw values;
-    std::string section, line;
-    while (std::getline(in, line)) {
-        bool quoted = false;
-        for (size_t i = 0; i < line.size(); ++i) {
-            if (line[i] == '"') quoted = !quoted;
-            else if (line[i] == '#' && !quoted) {
-                line = line.substr(0, i);
-                break;
-            }
-        }
-        const std::string t = strip(line);
-        if (t.empty()) continue;
-        if (t.front() == '[' && t.back() == ']') {
-            section = strip(t.substr(1, t.size() - 2));
-            continue;
-        }
-        const auto eq = t.find('=');
-        if (eq == std::string::npos)
-            throw std::runtime_error("Malformed config line (expected 'key = value'): " + line);
-        const std::string key = strip(t.substr(0, eq));
-        std::string value = strip(t.substr(eq + 1));
-        if (value.size() >= 2 && value.front() == '"' && value.back() == '"') value = value.substr(1, value.size() - 2);
-        values[section.empty() ? key : section + "." + key] = value;
-    }
-    return values;
-}
-
-double get_real(const Raw& c, const std::string& k, double fb) {
-    const auto it = c.find(k);
-    return it == c.end() ? fb : std::stod(it->second);
-}
-int get_int(const Raw& c, const std::string& k, int fb) {
-    const auto it = c.find(k);
-    return it == c.end() ? fb : std::stoi(it->second);
-}
-uint64_t get_u64(const Raw& c, const std::string& k, uint64_t fb) {
-    const auto it = c.find(k);
-    if (it == c.end()) return fb;
-    if (!it->second.empty() && it->second.front() == '-') throw std::runtime_error(k + " must not be negative");
-    return std::stoull(it->second);
-}
-bool get_bool(const Raw& c, const std::string& k, bool fb) {
-    const auto it = c.find(k);
-    if (it == c.end()) return fb;
-    if (it->second == "true") return true;
-    if (it->second == "false") return false;
-    throw std::runtime_error(k + " must be true or false");
-}
-std::string get_str(const Raw& c, const std::string& k, const std::string& fb) {
-    const auto it = c.find(k);
-    return it == c.end() ? fb : it->second;
-}
-
-// photon_generation.hpp:77-85
-int parse_generator(const std::string& name) {
-    if (name == "blackbody") return GRT_GEN_BLACKBODY;
-    if (name == "power-law" || name == "power_law" || name == "powerlaw") return GRT_GEN_POWER_LAW;
-    if (name == "custom") return GRT_GEN_CUSTOM;
-    throw std::runtime_error("photons.generator must be 'blackbody', 'power-law', or 'custom' (got '" + name + "')");
-}
-
-// The reference's validate() checks (toml_config.hpp:238-276,
-// photon_generation.hpp:26-74) as one function.
-void validate_or_throw(const grt_params& p) {
-    if (p.nphotons == 0 || p.nphotons > 100000000000ULL)
-        throw std::runtime_error("photons.count must be in [1, 100000000000]");
-    if (p.max_steps <= 0) throw std::runtime_error("integration.max_steps must be positive");
-    if (p.output_interval == 0) throw std::runtime_error("output.interval must be positive");
-    if (p.image_nx == 0 || p.image_ny == 0 || p.spectrum_bins == 0)
-        throw std::runtime_error("output image dimensions and spectrum_bins must be positive");
-    if (!(p.spectrum_min_hz > 0.0) || !(p.spectrum_max_hz > p.spectrum_min_hz))
-        throw std::runtime_error("output requires 0 < spectrum_min_hz < spectrum_max_hz");
-    if (!(p.camera_distance > 0.0) || !(p.camera_width > 0.0) || !(p.camera_height > 0.0))
-        throw std::runtime_error("camera distance, width, and height must be positive");
-    if (!std::isfinite(p.scattering_albedo) || p.scattering_albedo < 0.0 || p.scattering_albedo > 1.0)
-        throw std::runtime_error("scattering.albedo must be finite and in [0, 1]");
-    if (!std::isfinite(p.absorption_coefficient) || p.absorption_coefficient < 0.0)
-        throw std::runtime_error("radiative_transfer.absorption_coefficient must be finite and non-negative");
-    if (!std::isfinite(p.emission_coefficient) || p.emission_coefficient < 0.0)
-        throw std::runtime_error("radiative_transfer.emission_coefficient must be finite and non-negative");
-    if (p.termination_percent <= 0.0 || p.termination_percent > 1.0)
-        throw std::runtime_error("integration.termination_percent must be in (0, 1]");
-    if (!(p.superphoton_count_normalization > 0.0) || !std::isfinite(p.superphoton_count_normalization))
-        throw std::runtime_error("photons.superphoton_count_normalization must be finite and positive");
-    if (!(p.energy_per_cell_erg >= 0.0) || !std::isfinite(p.energy_per_cell_erg))
-        throw std::runtime_error("photons.energy_per_cell_erg must be finite and non-negative");
-    if (p.generator == GRT_GEN_POWER_LAW) {
-        if (!std::isfinite(p.power_law_slope)) throw std::runtime_error("photons.power_law_slope must be finite");
-        if (!(p.nu_min_hz > 0.0) || !(p.nu_max_hz > p.nu_min_hz) || !std::isfinite(p.nu_min_hz) ||
-            !std::isfinite(p.nu_max_hz))
-            throw std::runtime_error("power-law generation requires 0 < photons.nu_min_hz < photons.nu_max_hz");
-    }
-    if (p.generator == GRT_GEN_CUSTOM && (!(p.custom_frequency_hz > 0.0) || !std::isfinite(p.custom_frequency_hz)))
-        throw std::runtime_error("photons.custom_frequency_hz must be finite and positive");
-    const double units[6] = {p.length_cm_per_code, p.time_s_per_code, p.density_g_cm3_per_code,
-                             p.temperature_k_per_code, p.four_velocity_cm_s_per_code, p.magnetic_gauss_per_code};
-    for (double u : units)
-        if (!(u > 0.0) || !std::isfinite(u))
-            throw std::runtime_error("all [units] conversion factors must be finite and positive");
-    if (!(p.mass > 0.0)) throw std::runtime_error("black_hole.mass must be positive");
-    if (std::fabs(p.spin) > p.mass) throw std::runtime_error("black_hole.spin must satisfy |spin| <= mass");
-    if (p.mode != GRT_MODE_IMAGE && p.mode != GRT_MODE_DISK) throw std::runtime_error("simulation.mode must be 'image' or 'disk'");
-    if (p.integrator != GRT_RK4 && p.integrator != GRT_RK45)
-        throw std::runtime_error("integration.integrator must be \"rk4\" or \"rk45\"");
-    if (p.precision != GRT_PREC_FP64 && p.precision != GRT_PREC_MIXED)
-        throw std::runtime_error("precision must be GRT_PREC_FP64 or GRT_PREC_MIXED");
-}
+bool finite_positive(double v) { return std::isfinite(v) && v > 0.0; }
+bool finite_nonnegative(double v) { return std::isfinite(v) && v >= 0.0; }
 
 }  // namespace
 
@@ -214,127 +106,61 @@ grt_status grt_params_validate(const grt_params* p, char* err, size_t err_len) {
         set_err(err, err_len, "null params");
         return GRT_EINVAL;
     }
-    try {
-        validate_or_throw(*p);
-    } catch (const std::exception& e) {
-        set_err(err, err_len, e.what());
-        return GRT_EINVAL;
-    }
-    return GRT_OK;
-}
-
-grt_status grt_params_from_toml(const char* path, grt_params* p, char* numpy_dir, size_t numpy_dir_len,
-                                char* output_dir, size_t output_dir_len, char* name, size_t name_len,
-                                char* err, size_t err_len) {
-    if (!path || !p) {
-        set_err(err, err_len, "null argument");
-        return GRT_EINVAL;
-    }
-    grt_params q;
-    grt_params_default(&q);
-    try {
-        const Raw c = parse_flat(path);
-        const std::string mode = get_str(c, "simulation.mode", "image");
-        if (mode == "image") q.mode = GRT_MODE_IMAGE;
-        else if (mode == "disk") q.mode = GRT_MODE_DISK;
-        else throw std::runtime_error("simulation.mode must be 'image' or 'disk'");
-        const std::string sim_name = get_str(c, "simulation.name", "output");
-        const std::string npdir = get_str(c, "input.numpy_dir", ".");
-        q.scattering_enabled = get_bool(c, "scattering.enabled", false);
-        q.scattering_albedo = get_real(c, "scattering.albedo", q.scattering_albedo);
-        q.scattering_seed = get_u64(c, "scattering.seed", q.scattering_seed);
-        q.absorption_enabled = get_bool(c, "radiative_transfer.absorption_enabled", false);
-        q.emission_enabled = get_bool(c, "radiative_transfer.emission_enabled", false);
-        q.absorption_coefficient = get_real(c, "radiative_transfer.absorption_coefficient", 0.0);
-        q.emission_coefficient = get_real(c, "radiative_transfer.emission_coefficient", 0.0);
-        const std::string integ = get_str(c, "integration.integrator", "rk45");
-        if (integ == "rk4") q.integrator = GRT_RK4;
-        else if (integ == "rk45") q.integrator = GRT_RK45;
-        else throw std::runtime_error("integration.integrator must be \"rk4\" or \"rk45\"");
-        q.mass = get_real(c, "black_hole.mass", q.mass);
-        q.spin = get_real(c, "black_hole.spin", q.spin);
-        if (q.mass <= 0.0) throw std::runtime_error("black_hole.mass must be positive (got " + std::to_string(q.mass) + ")");
-        if (std::fabs(q.spin) > q.mass)
-            throw std::runtime_error("black_hole.spin must satisfy |spin| <= mass, i.e. dimensionless spin a/M in [-1, 1] (got spin=" +
-                                     std::to_string(q.spin) + ", mass=" + std::to_string(q.mass) +
-                                     "); |spin| > mass is a naked singularity.");
-        const double horizon = q.mass + std::sqrt(std::fmax(0.0, q.mass * q.mass - q.spin * q.spin));
-        q.camera_theta = get_real(c, "camera.theta", q.camera_theta);
-        q.camera_phi = get_real(c, "camera.phi", q.camera_phi);
-        q.camera_width = get_real(c, "camera.width", q.camera_width);
-        q.camera_height = get_real(c, "camera.height", q.camera_height);
-        q.camera_distance = get_real(c, "camera.distance", q.camera_distance);
-        q.nphotons = get_u64(c, "photons.count", q.nphotons);
-        q.generator = parse_generator(get_str(c, "photons.generator", "blackbody"));
-        q.superphoton_count_normalization = get_real(c, "photons.superphoton_count_normalization", q.superphoton_count_normalization);
-        q.energy_per_cell_erg = get_real(c, "photons.energy_per_cell_erg", q.energy_per_cell_erg);
-        q.power_law_slope = get_real(c, "photons.power_law_slope", q.power_law_slope);
-        q.nu_min_hz = get_real(c, "photons.nu_min_hz", q.nu_min_hz);
-        q.nu_max_hz = get_real(c, "photons.nu_max_hz", q.nu_max_hz);
-        q.custom_frequency_hz = get_real(c, "photons.custom_frequency_hz", q.custom_frequency_hz);
-        q.length_cm_per_code = get_real(c, "units.length_cm_per_code", q.length_cm_per_code);
-        q.time_s_per_code = get_real(c, "units.time_s_per_code", q.time_s_per_code);
-        q.density_g_cm3_per_code = get_real(c, "units.density_g_cm3_per_code", q.density_g_cm3_per_code);
-        q.temperature_k_per_code = get_real(c, "units.temperature_k_per_code", q.temperature_k_per_code);
-        q.four_velocity_cm_s_per_code = get_real(c, "units.four_velocity_cm_s_per_code", q.four_velocity_cm_s_per_code);
-        q.magnetic_gauss_per_code = get_real(c, "units.magnetic_gauss_per_code", q.magnetic_gauss_per_code);
-        q.max_steps = get_int(c, "integration.max_steps", static_cast<int>(q.max_steps));
-        q.termination_percent = get_real(c, "integration.termination_percent", q.termination_percent);
-        q.initial_step = get_real(c, "integration.initial_step", q.initial_step);
-        q.atol = get_real(c, "integration.atol", q.atol);
-        q.rtol = get_real(c, "integration.rtol", q.rtol);
-        q.r_term_min = get_real(c, "termination.r_min", horizon);
-        q.r_term_max = get_real(c, "termination.r_max", 1.5 * q.camera_distance);
-        q.output_interval = get_u64(c, "output.interval", q.output_interval);
-        const std::string outdir = get_str(c, "output.directory", "./output");
-        q.image_nx = get_u64(c, "output.image_nx", q.image_nx);
-        q.image_ny = get_u64(c, "output.image_ny", q.image_ny);
-        q.spectrum_bins = get_u64(c, "output.spectrum_bins", q.spectrum_bins);
-        q.spectrum_min_hz = get_real(c, "output.spectrum_min_hz", q.spectrum_min_hz);
-        q.spectrum_max_hz = get_real(c, "output.spectrum_max_hz", q.spectrum_max_hz);
-        if (npdir.empty()) throw std::runtime_error("input.numpy_dir must not be empty");
-        if (outdir.empty()) throw std::runtime_error("output.directory must not be empty");
-        if (sim_name.empty()) throw std::runtime_error("simulation.name must not be empty");
-        validate_or_throw(q);
-        set_str(numpy_dir, numpy_dir_len, npdir);
-        set_str(output_dir, output_dir_len, outdir);
-        set_str(name, name_len, sim_name);
-    } catch (const std::runtime_error& e) {
-        set_err(err, err_len, e.what());
-        return std::string(e.what()).rfind("Failed to open config file", 0) == 0 ? GRT_EIO : GRT_EINVAL;
-    } catch (const std::exception& e) {
-        set_err(err, err_len, std::string("invalid config value: ") + e.what());
-        return GRT_EINVAL;
-    }
-    *p = q;
-    return GRT_OK;
-}
-
-grt_status grt_output_options_from_toml(const char* path, char* variables, size_t variables_len, uint64_t* stride,
-                                        char* err, size_t err_len) {
-    if (!path) {
-        set_err(err, err_len, "null argument");
-        return GRT_EINVAL;
-    }
-    try {
-        const Raw c = parse_flat(path);
-        const std::string spec = get_str(c, "output.variables", "id,frequency,x0,x1,x2,x3,k0,k1,k2,k3,I,Q,U,V,phase");
-        const uint64_t st = get_u64(c, "output.stride", 1);
-        if (st == 0) throw std::runtime_error("output.stride must be positive");
-        std::vector<int> fields;
-        std::string msg;
-        if (!grt::parse_output_variables(spec, fields, msg)) throw std::runtime_error(msg);
-        if (variables && variables_len) {
-            if (spec.size() + 1 > variables_len) throw std::runtime_error("output.variables longer than the buffer");
-            set_str(variables, variables_len, spec);
+    const bool gen_ok = p->generator == GRT_GEN_BLACKBODY || p->generator == GRT_GEN_POWER_LAW ||
+                        p->generator == GRT_GEN_CUSTOM;
+    const bool power_law_ok = p->generator != GRT_GEN_POWER_LAW ||
+                              (std::isfinite(p->power_law_slope) && finite_positive(p->nu_min_hz) &&
+                               std::isfinite(p->nu_max_hz) && p->nu_max_hz > p->nu_min_hz);
+    const bool units_ok = finite_positive(p->length_cm_per_code) && finite_positive(p->time_s_per_code) &&
+                          finite_positive(p->density_g_cm3_per_code) && finite_positive(p->temperature_k_per_code) &&
+                          finite_positive(p->four_velocity_cm_s_per_code) &&
+                          finite_positive(p->magnetic_gauss_per_code);
+    const Rule rules[] = {
+        {p->mode == GRT_MODE_IMAGE || p->mode == GRT_MODE_DISK, "grt_params.mode: GRT_MODE_IMAGE or GRT_MODE_DISK"},
+        {p->integrator == GRT_RK4 || p->integrator == GRT_RK45, "grt_params.integrator: GRT_RK4 or GRT_RK45"},
+        {p->precision == GRT_PREC_FP64 || p->precision == GRT_PREC_MIXED,
+         "grt_params.precision: GRT_PREC_FP64 or GRT_PREC_MIXED"},
+        {gen_ok, "grt_params.generator: GRT_GEN_BLACKBODY, GRT_GEN_POWER_LAW or GRT_GEN_CUSTOM"},
+        {finite_positive(p->mass), "grt_params.mass: finite and positive"},
+        {std::isfinite(p->spin) && std::fabs(p->spin) <= p->mass,
+         "grt_params.spin: |spin| <= mass (a Kerr black hole, not a naked singularity)"},
+        {finite_nonnegative(p->r_term_min) && p->r_term_max > p->r_term_min,
+         "grt_params termination radii: 0 <= r_term_min < r_term_max"},
+        {finite_positive(p->atol) && finite_positive(p->rtol), "grt_params.atol, rtol: finite and positive"},
+        {finite_positive(p->min_step_scale) && p->min_step_scale <= 1.0 && std::isfinite(p->max_step_scale) &&
+             p->max_step_scale >= 1.0 && finite_positive(p->safety),
+         "grt_params step-size controller: 0 < min_step_scale <= 1 <= max_step_scale, safety > 0"},
+        {p->max_steps > 0, "grt_params.max_steps: positive"},
+        {p->termination_percent > 0.0 && p->termination_percent <= 1.0,
+         "grt_params.termination_percent: in (0, 1]"},
+        {p->output_interval > 0, "grt_params.output_interval: positive"},
+        {p->nphotons > 0, "grt_params.nphotons: positive (the count the terminated fraction is taken of)"},
+        {finite_positive(p->initial_step), "grt_params.initial_step: finite and positive"},
+        {finite_positive(p->camera_distance) && finite_positive(p->camera_width) &&
+             finite_positive(p->camera_height) && std::isfinite(p->camera_theta) && std::isfinite(p->camera_phi),
+         "grt_params camera: distance, width and height finite and positive, angles finite"},
+        {finite_nonnegative(p->absorption_coefficient) && finite_nonnegative(p->emission_coefficient),
+         "grt_params transfer coefficients: finite and non-negative"},
+        {finite_nonnegative(p->scattering_albedo) && p->scattering_albedo <= 1.0,
+         "grt_params.scattering_albedo: in [0, 1]"},
+        {finite_positive(p->superphoton_count_normalization),
+         "grt_params.superphoton_count_normalization: finite and positive"},
+        {finite_nonnegative(p->energy_per_cell_erg), "grt_params.energy_per_cell_erg: finite and non-negative"},
+        {power_law_ok, "grt_params power-law generator: finite slope and 0 < nu_min_hz < nu_max_hz"},
+        {p->generator != GRT_GEN_CUSTOM || finite_positive(p->custom_frequency_hz),
+         "grt_params.custom_frequency_hz: finite and positive for the custom generator"},
+        {units_ok, "grt_params unit scales: every *_per_code factor finite and positive"},
+        {p->image_nx > 0 && p->image_ny > 0 && p->spectrum_bins > 0,
+         "grt_params image_nx, image_ny, spectrum_bins: positive"},
+        {finite_positive(p->spectrum_min_hz) && std::isfinite(p->spectrum_max_hz) &&
+             p->spectrum_max_hz > p->spectrum_min_hz,
+         "grt_params spectrum range: 0 < spectrum_min_hz < spectrum_max_hz"},
+    };
+    for (const Rule& r : rules) {
+        if (!r.ok) {
+            set_err(err, err_len, r.message);
+            return GRT_EINVAL;
         }
-        if (stride) *stride = st;
-    } catch (const std::runtime_error& e) {
-        set_err(err, err_len, e.what());
-        return std::string(e.what()).rfind("Failed to open config file", 0) == 0 ? GRT_EIO : GRT_EINVAL;
-    } catch (const std::exception& e) {
-        set_err(err, err_len, std::string("invalid config value: ") + e.what());
-        return GRT_EINVAL;
     }
     return GRT_OK;
 }

@@ -52,8 +52,6 @@ def load(path: Path | None = None):
     L.grt_params_default.argtypes = [P(Params)]
     L.grt_params_default.restype = None
     L.grt_params_validate.argtypes = [P(Params), C.c_char_p, C.c_size_t]
-    L.grt_params_from_toml.argtypes = [C.c_char_p, P(Params), C.c_char_p, C.c_size_t, C.c_char_p,
-                                       C.c_size_t, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]
     L.grt_create.argtypes = [P(Params), P(vp)]
     L.grt_destroy.argtypes = [vp]
     L.grt_destroy.restype = None
@@ -98,8 +96,6 @@ def load(path: Path | None = None):
     L.grt_forward_checkpointed.argtypes = [vp, C.c_int64, P(RunStats)]
     L.grt_adjoint_image_I.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_double)]
     L.grt_parse_output_variables.argtypes = [C.c_char_p, P(C.c_int32), P(C.c_size_t), C.c_char_p, C.c_size_t]
-    L.grt_output_options_from_toml.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t, P(C.c_uint64), C.c_char_p,
-                                               C.c_size_t]
     L.grt_write_output_step_npz.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int64, C.c_int32, C.c_char_p, C.c_uint64]
     L.grt_run_with_output.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64, P(RunStats)]
     L.grt_get_all_batch_image_products.argtypes = [vp, P(ImageProducts), C.c_size_t]
@@ -112,10 +108,10 @@ def load(path: Path | None = None):
     L.grt_render_async.restype = C.c_int
     L.grt_render_wait.argtypes = [vp, P(RunStats)]
     L.grt_render_wait.restype = C.c_int
-    for name in ("grt_parse_output_variables", "grt_output_options_from_toml", "grt_write_output_step_npz",
+    for name in ("grt_parse_output_variables", "grt_write_output_step_npz",
                  "grt_run_with_output", "grt_set_cell_multipliers", "grt_forward_checkpointed", "grt_adjoint_image_I",
                  "grt_init_image_batch", "grt_get_batch_image_products", "grt_write_batch_products_npz",
-                 "grt_render_graph", "grt_trace_device_noalloc", "grt_measure_fma_peaks", "grt_params_validate", "grt_params_from_toml", "grt_create", "grt_set_params",
+                 "grt_render_graph", "grt_trace_device_noalloc", "grt_measure_fma_peaks", "grt_params_validate", "grt_create", "grt_set_params",
                  "grt_set_stream", "grt_synchronize", "grt_upload_grid", "grt_upload_grid_numpy_dir",
                  "grt_upload_photons", "grt_init_image_photons", "grt_init_image_photons_random", "grt_run",
                  "grt_download_photons",
@@ -149,34 +145,11 @@ def parse_output_variables(spec: str) -> list:
     return [OUTPUT_FIELDS[fields[k]] for k in range(count.value)]
 
 
-def output_options_from_toml(path) -> tuple:
-    """(output.variables, output.stride) of a reference TOML config."""
-    buf = C.create_string_buffer(4096)
-    stride = C.c_uint64(0)
-    err = C.create_string_buffer(512)
-    rc = load().grt_output_options_from_toml(str(path).encode(), buf, 4096, C.byref(stride), err, 512)
-    if rc != GRT_OK:
-        raise GrtError(rc, err.value.decode())
-    return buf.value.decode(), int(stride.value)
-
-
 def validate_params(p: Params):
     buf = C.create_string_buffer(512)
     rc = load().grt_params_validate(C.byref(p), buf, 512)
     if rc != GRT_OK:
         raise GrtError(rc, buf.value.decode())
-
-
-def params_from_toml(path):
-    """Parse a reference TOML file: returns (Params, numpy_dir, output_dir, name)."""
-    L = load()
-    p = Params()
-    bufs = [C.create_string_buffer(4096) for _ in range(4)]
-    rc = L.grt_params_from_toml(str(path).encode(), C.byref(p), bufs[0], 4096, bufs[1], 4096, bufs[2], 4096,
-                                bufs[3], 4096)
-    if rc != GRT_OK:
-        raise GrtError(rc, bufs[3].value.decode())
-    return p, bufs[0].value.decode(), bufs[1].value.decode(), bufs[2].value.decode()
 
 
 def measure_fma_peaks():

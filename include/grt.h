@@ -181,20 +181,11 @@ const char* grt_build_info(void);
 /* Fill p with the reference's compiled-in defaults (src/utils.cpp:4-37). */
 void grt_params_default(grt_params* p);
 
-/*
- * Parse a reference TOML config (same keys, defaults and validation as
- * toml_config::load_and_apply_toml_config, src/input/toml_config.hpp:129-278)
- * into p.  numpy_dir/output_dir/name receive input.numpy_dir, output.directory
- * and simulation.name (may be NULL).  On error returns GRT_EINVAL/GRT_EIO and
- * writes the message to err (if err_len > 0).
- */
-grt_status grt_params_from_toml(const char* path, grt_params* p,
-                                char* numpy_dir, size_t numpy_dir_len,
-                                char* output_dir, size_t output_dir_len,
-                                char* name, size_t name_len,
-                                char* err, size_t err_len);
-
-/* Validate p the way the reference's loader does; GRT_EINVAL on failure. */
+/* Check that p describes a run the kernels can trace (every mode, integrator and generator
+ * field known; masses, tolerances, radii, camera, scales and ranges finite and ordered);
+ * GRT_EINVAL and a message naming the field on failure.  grt_create and grt_set_params
+ * call it.  The reference's TOML config is read by the reference's own loader: its parsed
+ * structs reach grt_params through include/grt_reference_adapter.hpp. */
 grt_status grt_params_validate(const grt_params* p, char* err, size_t err_len);
 
 /* Create a context on the current CUDA device. */
@@ -332,16 +323,8 @@ grt_status grt_write_image_products_npz(grt_ctx* ctx, const char* output_dir, co
  * *count their number.  GRT_EINVAL with the
  * reference's message ("unknown output variable: X", "output variables cannot
  * be empty") otherwise.
- *
- * grt_output_options_from_toml reads output.variables (default
- * "id,frequency,x0,x1,x2,x3,k0,k1,k2,k3,I,Q,U,V,phase") and output.stride
- * (default 1, must be positive) of a reference TOML config
- * (toml_config.hpp:225-243), validating the selection.
  */
 grt_status grt_parse_output_variables(const char* spec, int32_t* fields, size_t* count, char* err, size_t err_len);
-grt_status grt_output_options_from_toml(const char* path, char* variables, size_t variables_len, uint64_t* stride,
-                                        char* err, size_t err_len);
-
 /*
  * write_output_step (write_output.hpp:90-103): <output_dir>/<name>_step_<step>_rank<rank>.npz
  * holding the selected fields of photons 0, stride, 2*stride, ... (each a 1-D

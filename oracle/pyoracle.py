@@ -188,6 +188,7 @@ class Reference:
         L = self.lib
         L.ref_last_error.restype = C.c_char_p
         L.ref_params_from_toml.argtypes = [C.c_char_p, C.POINTER(Params)]
+        L.ref_adapter_params_from_toml.argtypes = [C.c_char_p, C.POINTER(Params)]
         L.ref_init_image_photons.argtypes = [C.c_char_p, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(PhotonSoA)]
         L.ref_init_image_photons_random.argtypes = [C.c_char_p, C.c_uint64, C.c_uint64, C.POINTER(PhotonSoA)]
         L.ref_run_photons.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(PhotonSoA), C.c_uint64,
@@ -230,6 +231,14 @@ class Reference:
     def params_from_toml(self, path) -> Params:
         p = Params()
         if self.lib.ref_params_from_toml(str(path).encode(), C.byref(p)) != 0:
+            raise ValueError(self.error())
+        return p
+
+    def adapter_params_from_toml(self, path) -> Params:
+        """grt_params as the product's drop-in adapter maps the structs the
+        reference's own loader fills from this config."""
+        p = Params()
+        if self.lib.ref_adapter_params_from_toml(str(path).encode(), C.byref(p)) != 0:
             raise ValueError(self.error())
         return p
 

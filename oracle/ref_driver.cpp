@@ -29,6 +29,7 @@
 #include <sstream>
 
 #include "grt.h"
+#include "grt_reference_adapter.hpp"  // the product's drop-in mapping, checked below
 
 namespace {
 
@@ -179,6 +180,22 @@ int ref_params_from_toml(const char* toml_path, grt_params* p) {
     p->spectrum_bins = cfg.options.spectrum_bins;
     p->spectrum_min_hz = cfg.options.spectrum_min_hz;
     p->spectrum_max_hz = cfg.options.spectrum_max_hz;
+    return 0;
+}
+
+// The product's drop-in mapping (grt_adapter::params_from_reference in
+// include/grt_reference_adapter.hpp) of what the reference's loader fills,
+// with the models main() builds from it (src/main.cpp:246-266), to compare
+// with ref_params_from_toml.
+int ref_adapter_params_from_toml(const char* toml_path, grt_params* p) {
+    Loaded cfg;
+    if (!load_config(toml_path, cfg)) return 1;
+    *p = grt_adapter::params_from_reference(
+        cfg.options, cfg.generation, cfg.units,
+        ScatteringModel{cfg.options.enable_scattering, cfg.options.scattering_albedo, cfg.options.scattering_seed},
+        RadiativeTransferModel{cfg.options.enable_absorption, cfg.options.enable_emission,
+                               cfg.options.absorption_coefficient, cfg.options.emission_coefficient},
+        cfg.options.integrator, 0);
     return 0;
 }
 

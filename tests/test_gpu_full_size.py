@@ -21,7 +21,7 @@ import pytest
 
 import pyoracle
 from grt import config, torus, workloads
-from helpers import max_rel, run_gpu
+from helpers import FP64_RTOL, max_rel, run_gpu
 
 pytestmark = pytest.mark.gpu
 
@@ -35,8 +35,12 @@ def assert_bitwise(got, want):
 
 def assert_products(got, want):
     assert int(got.arrived_count[0]) == int(want.arrived_count[0])
+    # image pixels collect a few arrivals each; a spectrum bin collects
+    # thousands, summed by device atomics in another order than the
+    # reference's serial loop, so it is held to the 1e-9 parity bar
     for f in PRODUCT_FIELDS:
-        assert max_rel(getattr(got, f), getattr(want, f)) <= 1e-12, f
+        tol = FP64_RTOL if f == "spectrum_I" else 1e-12
+        assert max_rel(getattr(got, f), getattr(want, f)) <= tol, f
 
 
 @pytest.mark.parametrize("w", [workloads.C1, workloads.C2], ids=["c1_rk4_64px", "c2_rk45_256px"])

@@ -8,7 +8,7 @@ import pytest
 
 import pyoracle
 from grt import workloads
-from helpers import max_rel, mini
+from helpers import FP64_RTOL, max_rel, mini
 
 pytestmark = pytest.mark.gpu
 
@@ -40,7 +40,7 @@ def test_random_screen_rays_and_trace_match_oracle(gpu, oracle, rank):
     assert int(prod.arrived_count[0]) == int(ref_prod.arrived_count[0]) > 0
     assert prod.image_I.shape == (p.image_ny, p.image_nx)
     for f in ("image_I", "image_Q", "image_U", "image_V", "spectrum_I"):
-        assert max_rel(getattr(prod, f), getattr(ref_prod, f)) <= 1e-12, f
+        assert max_rel(getattr(prod, f), getattr(ref_prod, f)) <= (FP64_RTOL if f == "spectrum_I" else 1e-12), f
     if rank:
         # another rank draws other screen positions
         other = oracle.init_image_photons_random(mini(workloads.C2, 16, (32, 16, 16)).params(), n, id_offset=11)

@@ -1,13 +1,12 @@
 """Output-step selection (OutputSelection::parse, src/output/output_variables.hpp:
-27-70) and the output keys of the TOML config (toml_config.hpp:225-243): the
-library's parser against the reference's own parser (compiled from the
-reference tree, oracle/_ref) on hand-written and random specifications,
-errors included."""
+27-70): the library's parser against the reference's own parser (compiled
+from the reference tree, oracle/_ref) on hand-written and random
+specifications, errors included."""
 
 import numpy as np
 import pytest
 
-from grt import config, lib, workloads
+from grt import lib
 from grt.lib import GrtError, OUTPUT_FIELDS
 
 SPECS = [
@@ -54,29 +53,3 @@ def test_selection_matches_reference(reference, spec):
 def test_random_selections_match_reference(reference):
     for spec in random_specs(400):
         assert ours(spec) == theirs(reference, spec), spec
-
-
-def test_output_options_from_toml(tmp_path):
-    p = workloads.C1.params()
-    text = config.toml_text(p, str(tmp_path / "np"), str(tmp_path / "out"), "run")
-    path = tmp_path / "c.toml"
-    path.write_text(text)
-    spec, stride = lib.output_options_from_toml(path)
-    assert lib.parse_output_variables(spec) == ["id", "frequency", "x0", "x1", "x2", "x3", "k0", "k1", "k2", "k3",
-                                                "I", "Q", "U", "V", "terminate", "phase"]
-    assert stride == 1
-    path.write_text(text.replace("stride = 1", "stride = 7").replace(
-        'variables = ["id"', 'variables = ["dlambda", "id"'))
-    spec, stride = lib.output_options_from_toml(path)
-    assert stride == 7 and lib.parse_output_variables(spec)[:2] == ["dlambda", "id"]
-    # defaults when the keys are absent
-    path.write_text("\n".join(l for l in text.splitlines() if not l.startswith(("stride", "variables"))) + "\n")
-    spec, stride = lib.output_options_from_toml(path)
-    assert stride == 1 and spec == lib.DEFAULT_OUTPUT_VARIABLES
-    for bad, msg in (("stride = 0", "output.stride must be positive"),
-                     ('variables = "x0, nope"', "unknown output variable: nope")):
-        lines = [l for l in text.splitlines() if not l.startswith(("stride", "variables"))]
-        lines.insert(lines.index("[output]") + 1, bad)
-        path.write_text("\n".join(lines) + "\n")
-        with pytest.raises(GrtError, match=msg):
-            lib.output_options_from_toml(path)
