@@ -246,6 +246,22 @@ def run_ours(args):
     world, rank, local = dist_setup(args.gpus)
     w = workloads.WORKLOADS[args.workload]
     bw = workloads.BATCHES[args.workload]
+    # N GPUs: a camera orbit of N frames (camera_phi = 2 pi k / N; the torus
+    # and the metric are axisymmetric, so every frame costs the same), whole
+    # frames assigned to ranks by shard_images -- the per-image partition of
+    # the multi-GPU design -- and every step ends with an all-gather of the
+    # frames' image products over NCCL.  One GPU renders frame 0, the workload.
+    from grt import parallel
+    frame_phis = [2.0 * math.pi * k / world for k in range(world)]
+    my_frames = parallel.shard_images([1.0] * world, world)[rank]
+    assert len(my_frames) == 1
+    frame_phi = frame_phis[my_frames[0]]
+
+    def frame_params(wl):
+        q = wl.params()
+        q.camera_phi = q.camera_phi + frame_phi
+        return q
+
     if args.images:
         # a slice of the batch (its first N images), for profiling runs
         bw = workloads.BatchWorkload(f"{bw.name}_first{args.images}", bw.base, bw.images[:args.images])
@@ -268,13 +284,13 @@ def run_ours(args):
     forms = {}
     for name in wanted:
         prec, batched = FORMS[name]
-        p = (bw if batched else w).params()
+        p = frame_params(bw if batched else w)
         p.precision = prec
         ctx = lib.Context(p)
         ctx.set_stream(stream.cuda_stream)
         ctx.upload_grid(grid)
         forms[name] = (ctx, batched)
-    specs = bw.specs()
+    specs = bw.specs(frame_params(bw))
 
     def prepare(ctx, batched):
         if batched:
@@ -301,11 +317,27 @@ def run_ours(args):
 
     results = {}
     images = {}
+    gathered_ok = {}
     sampler = ClockSampler(local).__enter__()
     for name, (ctx, batched) in forms.items():
         prepare(ctx, batched)
+        gather = None
+        if world > 1:
+            import torch.distributed as dist
+            nbytes = ctx.products_block_bytes
+            mine = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+            every = torch.empty(world * nbytes, dtype=torch.uint8, device="cuda")
+
+            def gather():
+                # this rank's frame products, device to device, then every
+                # rank's frames on every rank (NCCL), ordered on `stream`
+                ctx.copy_products_block(mine.data_ptr(), nbytes)
+                with torch.cuda.stream(stream):
+                    dist.all_gather_into_tensor(every, mine)
         for _ in range(args.warmup):
             ctx.render_graph()  # graph: init rays, trace, every image's products
+            if gather:
+                gather()
         torch.cuda.synchronize()
         barrier(world)
         total_ms = 0.0
@@ -319,6 +351,8 @@ def run_ours(args):
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev0.record(stream)
             st = ctx.render_graph()
+            if gather:
+                gather()
             ev1.record(stream)
             ev1.synchronize()
             total_ms += ev0.elapsed_time(ev1)
@@ -329,6 +363,9 @@ def run_ours(args):
             stats_acc = st
         sampler.timed(False)
         torch.cuda.synchronize()
+        if gather:
+            # the gathered block of this rank equals its own products
+            gathered_ok[name] = bool(torch.equal(every[rank * nbytes:(rank + 1) * nbytes], mine))
         barrier(world)
         total_ms = max_over_ranks(total_ms, world)
         n_rays = bw.rays if batched else w.pixels * w.pixels
@@ -524,7 +561,10 @@ def run_ours(args):
                        "rays_per_step": H["rays"], "geodesics_per_step": H["geodesics"],
                        "channel_sharing": bool(batched and H["geodesics"] < H["rays"]),
                        "l2": "flushed by a 256 MB device write before every timed step (outside the events)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": (f"frames x{world}: a camera orbit (camera_phi = 2 pi k / {world}), one "
+                                       "frame per GPU (shard_images), image products all-gathered over NCCL every "
+                                       "step inside the timed region" if world > 1 else "one GPU"),
+                       "frames": world},
             "forms": {k: {"rays_per_step": v["rays"], "rays_per_s": v["rays_per_s"],
                           "geodesics_per_step": v["geodesics"], "geodesics_per_s": v["geodesics_per_s"],
                           "rk_steps_per_s": v["rk_steps_per_s"],
@@ -548,6 +588,7 @@ def run_ours(args):
             "e2e": e2e,
             "e2e_serial": e2e_serial,
             "gpu_launches": H["launches"],
+            "products_gather_check": gathered_ok or None,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,

@@ -948,11 +948,11 @@ void fill_spectrum_frequencies(const grt_params& p, double* out) {
     }
 }
 
-// Per-warp loop limit of a trace launch (GRT_ETIMEOUT beyond it): every
-// photon may take `budget` calls of at most 13 attempts each.
-// Per-warp loop limit of a trace launch: the launch shape's max_iterations
-// when set, else a bound no launch that makes progress reaches (every warp
-// iteration is one RK45 attempt or RK4 step of at least one lane).
+// Per-warp loop limit of a trace launch (GRT_ETIMEOUT beyond it): the launch
+// shape's max_iterations
+// when set, else a bound no launch that makes progress reaches: every photon
+// may take `budget` calls of at most 13 attempts each, and every warp
+// iteration is one RK45 attempt or RK4 step of at least one lane.
 unsigned long long iteration_limit(const grt_ctx* c, const grt::KParams& kp, unsigned long long total, int blocks,
                                    int threads) {
     if (c->lc.max_iterations > 0) return static_cast<unsigned long long>(c->lc.max_iterations);
@@ -1190,6 +1190,35 @@ grt_status grt_get_batch_image_products(grt_ctx* c, size_t image, grt_image_prod
     st = enqueue_batch_products(c, image, out, c->stream);
     if (st != GRT_OK) return st;
     GRT_CUDA(c, cudaStreamSynchronize(c->stream), "products");
+    return GRT_OK;
+}
+
+size_t grt_products_block_bytes(const grt_ctx* c) {
+    if (!c || !c->have_images) return 0;
+    size_t values = c->images.size() * (c->p.spectrum_bins + 1);
+    for (const grt_image_spec& sp : c->images) values += 4 * sp.nx * sp.ny;
+    return values * sizeof(double);
+}
+
+grt_status grt_copy_products_block(grt_ctx* c, void* dst, size_t bytes) {
+    if (c && c->render_pending) return rendering(c);
+    if (!c || !dst) return GRT_EINVAL;
+    if (!c->have_images) return fail(c, GRT_ESTATE, "no image set (grt_init_image_photons or grt_init_image_batch)");
+    if (bytes < grt_products_block_bytes(c)) return fail(c, GRT_EINVAL, "dst is smaller than grt_products_block_bytes");
+    if (!c->bproducts_valid) {
+        grt_status st = launch_all_products(c);
+        if (st != GRT_OK) return st;
+        c->bproducts_valid = true;
+    }
+    const size_t nimg = c->images.size(), bins = c->p.spectrum_bins;
+    char* d = static_cast<char*>(dst);
+    const size_t img_bytes = c->bimage_off[nimg] * sizeof(double), spec_bytes = nimg * bins * sizeof(double);
+    GRT_CUDA(c, cudaMemcpyAsync(d, c->bimage.ptr, img_bytes, cudaMemcpyDefault, c->stream), "copy products");
+    if (spec_bytes)
+        GRT_CUDA(c, cudaMemcpyAsync(d + img_bytes, c->bspectrum.ptr, spec_bytes, cudaMemcpyDefault, c->stream),
+                 "copy products");
+    GRT_CUDA(c, cudaMemcpyAsync(d + img_bytes + spec_bytes, c->barrived.ptr, nimg * sizeof(unsigned long long),
+                                cudaMemcpyDefault, c->stream), "copy products");
     return GRT_OK;
 }
 

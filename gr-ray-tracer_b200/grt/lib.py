@@ -71,6 +71,10 @@ def load(path: Path | None = None):
     L.grt_photon_count.restype = C.c_size_t
     L.grt_geodesic_count.argtypes = [vp]
     L.grt_geodesic_count.restype = C.c_uint64
+    L.grt_products_block_bytes.argtypes = [vp]
+    L.grt_products_block_bytes.restype = C.c_size_t
+    L.grt_copy_products_block.argtypes = [vp, vp, C.c_size_t]
+    L.grt_copy_products_block.restype = C.c_int
     L.grt_get_image_products.argtypes = [vp, P(ImageProducts)]
     L.grt_write_image_products_npz.argtypes = [vp, C.c_char_p, C.c_char_p]
     L.grt_get_launch_config.argtypes = [vp, P(LaunchConfig)]
@@ -351,6 +355,15 @@ class Context:
     @property
     def n(self):
         return int(self.lib.grt_photon_count(self._h))
+
+    @property
+    def products_block_bytes(self):
+        return int(self.lib.grt_products_block_bytes(self._h))
+
+    def copy_products_block(self, dst_ptr: int, nbytes: int):
+        """Enqueue a copy of every image's products into dst_ptr (device or host
+        memory; see grt_copy_products_block) on the context's stream."""
+        self._check(self.lib.grt_copy_products_block(self._h, C.c_void_p(dst_ptr), nbytes))
 
     @property
     def geodesics(self):

@@ -5,9 +5,10 @@ grid (<= 55 MB) is replicated on each GPU.  The reference's MPI photon
 exchange (photon_exchange.hpp) exists only because its ranks own grid slabs.
 Two ways to use N GPUs:
 
-* replicas / images: each rank traces its own images (shard_images assigns
+* whole images: each rank traces its own images (shard_images assigns
   whole images to ranks, balancing rays); the only communication is gathering
-  the products, once, at the end;
+  the products (all_gather_blocks; bench.py --gpus N renders one frame of a
+  camera orbit per GPU and all-gathers the frames' products every step);
 * one image split by pixel rows: row_range gives rank r its rows
   (grt_init_image_rows), every rank bins its arrivals into the full image and
   reduce_products sums the products over the ranks -- the analogue of the
@@ -92,3 +93,19 @@ def _unflat(prod, flat: np.ndarray):
     prod.spectrum_I[...] = flat[o:o + b]
     o += b
     prod.arrived_count[...] = np.round(flat[o:o + 1]).astype(np.uint64)
+
+
+def all_gather_blocks(block, group=None) -> list:
+    """Every rank's block of equal size, in rank order, on every rank: the
+    gather of image products when whole images are owned by single ranks.
+    `block` is a 1-D numpy array or torch tensor; on NCCL it is staged
+    through the current CUDA device.  Returns numpy arrays."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    t = block if isinstance(block, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(block))
+    if dist.get_backend(group) == "nccl":
+        t = t.cuda()
+    parts = [torch.empty_like(t) for _ in range(dist.get_world_size(group))]
+    dist.all_gather(parts, t, group=group)
+    return [x.cpu().numpy() for x in parts]

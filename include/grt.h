@@ -406,6 +406,20 @@ grt_status grt_get_batch_image_products(grt_ctx* ctx, size_t image, grt_image_pr
  * = grt_batch_image_count): the copies of all images and one synchronisation. */
 grt_status grt_get_all_batch_image_products(grt_ctx* ctx, grt_image_products* outs, size_t nimages);
 
+/*
+ * The image products of the current image set (single image or batch) as one
+ * block, for collectives and device-side consumers (no counterpart in the
+ * reference, whose products go through host vectors and MPI_Reduce,
+ * write_output.hpp:109-127): every image's image_I, image_Q, image_U, image_V
+ * ([ny_k][nx_k] float64 each) in image order, then every image's spectrum_I
+ * ([spectrum_bins] float64), then every image's arrived count (uint64).  The
+ * products of the last render are used, or built first.  dst may be device or
+ * host memory; the copies are enqueued on the context's stream and the
+ * caller synchronises with it.
+ */
+size_t grt_products_block_bytes(const grt_ctx* ctx);
+grt_status grt_copy_products_block(grt_ctx* ctx, void* dst, size_t bytes);
+
 /* Write <output_dir>/<name>_image<k>_image_products.npz for every image k. */
 grt_status grt_write_batch_products_npz(grt_ctx* ctx, const char* output_dir, const char* name);
 
@@ -509,9 +523,15 @@ typedef struct grt_device_grid {
  * with GRT_EINVAL and a message), FP64 precision only.  Each call checks the
  * grid's separability on the device (one pass over the coordinate arrays),
  * then reads the axes back and derives the lookup's acceptance bounds on the
- * host with the routine grt_upload_grid uses, so results equal the context
- * entry point's bit for bit, cell edges included; the call waits for that
- * read-back and for the trace on `stream` before it returns.  The first call
+ * host with the routine grt_upload_grid uses, so the lookup accepts and
+ * rejects exactly what the context entry point's does, cell edges included.
+ * The grid stays in the reference's raw layout, so each sample's spherical
+ * four-velocity and field are turned Cartesian with the GPU's sin/cos (the
+ * context entry point precomputes them with the host's): results equal the
+ * context entry point's bit for bit without scattering, and in distribution
+ * with it, where an ulp in the fluid frame changes a scattered direction.
+ * The call waits for the read-back and for the trace on `stream` before it
+ * returns.  The first call
  * on a device looks up the scratch address (cudaGetSymbolAddress) with that
  * device current; make it before any stream capture.  err receives a message
  * on failure (may be NULL).  When a launch runs out of iterations the call

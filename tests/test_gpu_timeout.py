@@ -36,7 +36,7 @@ def test_iteration_limit_runs_out_and_the_run_resumes(gpu, split, form):
     assert fst["timed_out"] == 0 and fst["n_terminated"] == full.n
     ctx = gpu.Context(p)
     try:
-        ctx.set_launch_config(split_legs=split, max_iterations=60)
+        ctx.set_launch_config(split_legs=split, max_iterations=20)
         ctx.upload_grid(grid)
         ctx.init_image_photons(24, 24)
         rc, st = raw_run(ctx)

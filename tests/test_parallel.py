@@ -91,3 +91,60 @@ def test_row_sharded_image_reduces_to_single_process(tmp_path):
     a0, a1 = np.load(tmp_path / "all_0.npy"), np.load(tmp_path / "all_1.npy")
     assert np.array_equal(a0, a1)
     assert np.allclose(a0, r["want_image_I"], rtol=1e-12, atol=0.0)
+
+
+IMAGES = [15.0, 40.0, 60.0, 80.0, 30.0]  # inclinations of a small batch, one image each
+
+
+def _images_rank_main(rank, world, port, out_dir):
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    for p in (str(root / "gr-ray-tracer_b200"), str(root / "oracle"), str(root / "tests")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import math
+    import pyoracle
+    from grt import parallel as par
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        o = pyoracle.Oracle()
+        grid = W.torus()
+        shards = par.shard_images([W.pixels ** 2] * len(IMAGES), world)
+        slots = max(len(sh) for sh in shards)
+
+        def products_of(k):
+            p = W.params()
+            p.camera_theta = math.radians(IMAGES[k])
+            ph = o.init_image_photons(p, W.pixels, W.pixels)
+            o.run(p, grid, ph)
+            return par._flat(o.image_products(p, ph))
+
+        size = products_of(0).size
+        block = np.zeros(slots * size)
+        for j, k in enumerate(shards[rank]):
+            block[j * size:(j + 1) * size] = products_of(k)
+        parts = par.all_gather_blocks(block)
+        if rank == 0:
+            got = np.zeros((len(IMAGES), size))
+            for r, sh in enumerate(shards):
+                for j, k in enumerate(sh):
+                    got[k] = parts[r][j * size:(j + 1) * size]
+            want = np.stack([products_of(k) for k in range(len(IMAGES))])
+            np.savez(os.path.join(out_dir, "images.npz"), got=got, want=want)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_images_gather_to_single_process(tmp_path):
+    """Whole images assigned to two ranks by shard_images, each rank's
+    products gathered on every rank: rank 0 reassembles every image equal to
+    the single-process run."""
+    world = 2
+    mp.start_processes(_images_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    r = np.load(tmp_path / "images.npz")
+    assert np.array_equal(r["got"], r["want"])
+    assert (r["want"] != 0).any(axis=1).all()

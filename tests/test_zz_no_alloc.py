@@ -21,6 +21,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import pyoracle
 from grt import abi, workloads
 from helpers import assert_photons_match, mini, run_gpu
 
@@ -106,14 +107,7 @@ def test_noalloc_non_separable_grid(gpu, oracle):
     assert (want.phase == 3).sum() > 20  # rays arrived through the fluid
 
 
-def test_noalloc_disk_mode_with_scattering(gpu):
-    """Disk-mode packets from every cell, RK45, Thomson scattering on (Philox
-    draws keyed by packet id and step): photon for photon the same as the
-    context entry point."""
-    torch = pytest.importorskip("torch")
-    wd = workloads.DiskWorkload("disk_small", (32, 16, 16), 0.9, 6.0, max_steps=4000)
-    p = wd.params()
-    grid = wd.torus()
+def _disk_packets(gpu, p, grid):
     ctx = gpu.Context(p)
     try:
         ctx.upload_grid(grid)
@@ -123,8 +117,60 @@ def test_noalloc_disk_mode_with_scattering(gpu):
         ctx.close()
     assert n > 500
     p.nphotons = n
+    return init
+
+
+def test_noalloc_disk_mode_without_scattering(gpu):
+    """Disk-mode packets from every cell, RK45, absorption and emission:
+    photon for photon the same as the context entry point."""
+    torch = pytest.importorskip("torch")
+    wd = workloads.DiskWorkload("disk_small", (32, 16, 16), 0.9, 6.0, max_steps=4000)
+    p = wd.params()
+    p.scattering_enabled = 0
+    grid = wd.torus()
+    init = _disk_packets(gpu, p, grid)
     want = _twice_against_context(gpu, torch, p, grid, init, exact=True)
     assert (want.I != init.I).any()
+
+
+def test_noalloc_disk_mode_with_scattering(gpu):
+    """With Thomson scattering on, the allocation-free entry point reads the
+    reference's raw grid layout and turns each sample's spherical four-vectors
+    Cartesian with the GPU's sin/cos, where the context entry point uses
+    vectors precomputed with the host's; an ulp in the fluid frame changes a
+    scattered direction, so packets agree with the context entry point's in
+    distribution (escape fraction, escape energy and direction), and each of
+    the two calls in a row gives the same packets."""
+    torch = pytest.importorskip("torch")
+    scipy_stats = pytest.importorskip("scipy.stats")
+    wd = workloads.DiskWorkload("disk_small", (32, 16, 16), 0.9, 6.0, max_steps=4000)
+    p = wd.params()
+    grid = wd.torus()
+    init = _disk_packets(gpu, p, grid)
+    want, _, _ = run_gpu(gpu, p, grid, photons=init)
+    dgrid, G = _device_grid(torch, grid)
+    runs = []
+    for _ in range(2):
+        tensors, soa = _device_soa(torch, init)
+        torch.cuda.synchronize()
+        st = gpu.trace_device_noalloc(p, G, soa, init.n)
+        torch.cuda.synchronize()
+        runs.append(_to_host(tensors, init.n))
+        assert st["n_terminated"] == init.n
+    d = pyoracle.compare_photons(runs[0], runs[1])
+    assert all(v == 0 for v in d.values()), d
+
+    def escapes(ph):
+        r = np.sqrt(ph.x1 ** 2 + ph.x2 ** 2 + ph.x3 ** 2)
+        esc = (ph.phase == 4) & (r > p.r_term_max)
+        return esc, -ph.k0[esc], ph.x3[esc] / r[esc]
+
+    (e1, E1, c1), (e2, E2, c2) = escapes(runs[0]), escapes(want)
+    n = init.n
+    f1, f2 = e1.mean(), e2.mean()
+    assert abs(f1 - f2) <= 4 * np.sqrt(f1 * (1 - f1) / n + f2 * (1 - f2) / n) + 1e-12, (f1, f2)
+    assert scipy_stats.ks_2samp(E1, E2).pvalue > 0.01
+    assert scipy_stats.ks_2samp(c1, c2).pvalue > 0.01
 
 
 def test_noalloc_samples_at_radial_cell_edges(gpu):
