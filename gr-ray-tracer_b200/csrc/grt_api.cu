@@ -152,7 +152,7 @@ struct grt_ctx {
     DevBuf<unsigned long long> arrived;
     DevBuf<unsigned long long> scratch_u64;
     unsigned long long* host_u64 = nullptr;  // pinned
-    grt_launch_config lc{128, 4, 8, 32, 1, 0, 0};
+    grt_launch_config lc{128, 0, 8, 32, 1, 0, 0};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // images of the last grt_init_image_photons (one, cameras from p) or
     // grt_init_image_batch call; image k owns photon slots
@@ -456,8 +456,9 @@ grt_status grt_set_launch_config(grt_ctx* c, const grt_launch_config* cfg) {
     if (!c || !cfg) return GRT_EINVAL;
     if (cfg->threads_per_block != 128)
         return fail(c, GRT_EINVAL, "threads_per_block must be 128 (the trace kernels' block size)");
-    if (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 4)
-        return fail(c, GRT_EINVAL, "blocks_per_sm must be 2, 3 or 4 (register caps 255, 170, 128)");
+    if (cfg->blocks_per_sm != 0 && (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 4))
+        return fail(c, GRT_EINVAL,
+                    "blocks_per_sm must be 0 (automatic), 2, 3 or 4 (register caps 255, 170, 128)");
     if (cfg->refill_threshold < 1 || cfg->refill_threshold > 32)
         return fail(c, GRT_EINVAL, "refill_threshold must be in [1, 32]");
     if (cfg->photons_per_grab < 1 || cfg->photons_per_grab > (1 << 20))
@@ -978,24 +979,36 @@ grt_status prepare_trace_buffers(grt_ctx* c, unsigned long long queue) {
 // backward-leg launch, the packet generation of the rays it stopped at their
 // first fluid contact, and, with the queue head reset, the forward-leg launch
 // over the same queue.
+// Resident trace blocks per SM: the launch shape's, or with 0 (automatic)
+// the fewest of 2, 3, 4 that keep every geodesic of the queue resident at
+// once -- fewer blocks give each thread more registers (255, 170, 128) and
+// spill less, and a workload that fits needs no more lanes.
+int trace_blocks_per_sm(const grt_ctx* c, unsigned long long queue) {
+    if (c->lc.blocks_per_sm) return c->lc.blocks_per_sm;
+    for (int b = 2; b < 4; ++b)
+        if (static_cast<unsigned long long>(c->sm_count) * b * 128 >= queue) return b;
+    return 4;
+}
+
 cudaError_t launch_trace(const grt_ctx* c, const grt::KParams& kp, size_t smem) {
+    const int bps = trace_blocks_per_sm(c, kp.n);
     const grt_params& p = c->p;
     const bool mixed = p.precision == GRT_PREC_MIXED;
     if (!split_legs(c)) {
         // disk mode: the whole-ray kernel without the image-mode code (leg 3)
         const int leg = p.mode == GRT_MODE_DISK && kp.ngroups == 0 ? 3 : 0;
-        return grt::launch_trace(kp, mixed, leg, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+        return grt::launch_trace(kp, mixed, leg, p.integrator, c->sm_count, bps, smem, c->stream);
     }
     cudaError_t e = cudaMemsetAsync(kp.calls_carry, 0, kp.n * sizeof(long long), c->stream);
     if (e == cudaSuccess)
-        e = grt::launch_trace(kp, mixed, 1, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+        e = grt::launch_trace(kp, mixed, 1, p.integrator, c->sm_count, bps, smem, c->stream);
     if (e == cudaSuccess)
         e = grt::launch_generate_pending(
             kp, c->sm_count,
             grt::dev_trace_smem_bytes(0, 128, c->fluid_available && c->separable, c->nr, c->nth, c->nph), c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(&kp.counters->queue_head, 0, sizeof(unsigned long long), c->stream);
     if (e == cudaSuccess)
-        e = grt::launch_trace(kp, mixed, 2, p.integrator, c->sm_count, c->lc.blocks_per_sm, smem, c->stream);
+        e = grt::launch_trace(kp, mixed, 2, p.integrator, c->sm_count, bps, smem, c->stream);
     return e;
 }
 
@@ -1274,7 +1287,7 @@ grt_status run_steps(grt_ctx* c, grt_run_stats* stats, const OutputPlan* plan) {
     }
     const int threads = 128;
     const size_t smem = trace_smem(c);
-    const int blocks = c->sm_count * c->lc.blocks_per_sm;
+    const int blocks = c->sm_count * trace_blocks_per_sm(c, kp.n);
     const unsigned long long total = c->n;
     unsigned long long terminated = c->initial_terminated;
     const uint64_t interval = p.output_interval ? p.output_interval : 1;
@@ -1384,7 +1397,7 @@ grt_status grt_render_graph(grt_ctx* c, grt_run_stats* stats) {
         }
         kp.step0 = 0;
         kp.budget = p.max_steps;
-        kp.max_iterations = iteration_limit(c, kp, c->n, c->sm_count * c->lc.blocks_per_sm, 128);
+        kp.max_iterations = iteration_limit(c, kp, c->n, c->sm_count * trace_blocks_per_sm(c, kp.n), 128);
         const size_t smem = trace_smem(c);
         GRT_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed), "begin capture");
         grt_status gs = launch_image_inits(c);
@@ -1448,7 +1461,7 @@ static grt_status enqueue_render(grt_ctx* c, const grt_photon_soa* s, grt_image_
     kp.calls_carry = c->calls_carry.ptr;
     kp.step0 = 0;
     kp.budget = c->p.max_steps;
-    kp.max_iterations = iteration_limit(c, kp, n, c->sm_count * c->lc.blocks_per_sm, 128);
+    kp.max_iterations = iteration_limit(c, kp, n, c->sm_count * trace_blocks_per_sm(c, kp.n), 128);
     GRT_CUDA(c, cudaMemcpyAsync(c->ph.block.ptr, s->id, grt_photon_block_bytes(n), cudaMemcpyHostToDevice,
                                 c->copy_stream), "H2D photons");
     GRT_CUDA(c, cudaEventRecord(c->ev_uploaded, c->copy_stream), "event");

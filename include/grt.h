@@ -154,11 +154,12 @@ typedef struct grt_image_products {
     uint64_t* arrived_count;      /* [1] */
 } grt_image_products;
 
-/* Launch shape of the trace kernel: the library's default is {128, 4, 8, 32, 1, 0, 0};
+/* Launch shape of the trace kernel: the library's default is {128, 0, 8, 32, 1, 0, 0};
  * grt/autotune.py times the candidates on a workload and picks one. */
 typedef struct grt_launch_config {
     int32_t threads_per_block;    /* 128 (the trace kernels' block size) */
-    int32_t blocks_per_sm;        /* 2, 3 or 4 resident blocks per SM: register caps 255 / 170 / 128 */
+    int32_t blocks_per_sm;        /* 2, 3 or 4 resident blocks per SM: register caps 255 / 170 / 128;
+                                     0 = automatic: the fewest that keep every geodesic resident */
     int32_t refill_threshold;     /* idle lanes in a warp before it pulls new photons (1..32) */
     int32_t photons_per_grab;     /* photons a warp claims per access to the global queue */
     int32_t split_legs;           /* image mode: 1 = the backward legs, the packet generation at first
