@@ -331,7 +331,10 @@ grt::KParams make_kparams(const grt_ctx* c) {
     k.fp64_axis_sin2 = 0.01;
     // FP32 right-hand side for RK45 calls outside the fluid grid (lookup can
     // never accept radii above r_reject_hi); without a grid, everywhere.
-    k.fp32_min_radius_sq = c->fluid_available ? (std::isfinite(c->r_reject_hi) ? c->r_reject_hi * c->r_reject_hi : INFINITY) : 0.0;
+    // (GRT_PREC_MIXED_GRID: inside the grid too, after emission)
+    k.fp32_min_radius_sq = c->fluid_available && p.precision != GRT_PREC_MIXED_GRID
+                               ? (std::isfinite(c->r_reject_hi) ? c->r_reject_hi * c->r_reject_hi : INFINITY)
+                               : 0.0;
     k.renormalize = 1;
     k.rcp_ok = grt::rcp_params_ok(p.spin, p.mass);
     return k;
@@ -993,7 +996,7 @@ int trace_blocks_per_sm(const grt_ctx* c, unsigned long long queue) {
 cudaError_t launch_trace(const grt_ctx* c, const grt::KParams& kp, size_t smem) {
     const int bps = trace_blocks_per_sm(c, kp.n);
     const grt_params& p = c->p;
-    const bool mixed = p.precision == GRT_PREC_MIXED;
+    const bool mixed = p.precision != GRT_PREC_FP64;
     if (!split_legs(c)) {
         // disk mode: the whole-ray kernel without the image-mode code (leg 3)
         const int leg = p.mode == GRT_MODE_DISK && kp.ngroups == 0 ? 3 : 0;

@@ -118,8 +118,8 @@ grt_status grt_params_validate(const grt_params* p, char* err, size_t err_len) {
     const Rule rules[] = {
         {p->mode == GRT_MODE_IMAGE || p->mode == GRT_MODE_DISK, "grt_params.mode: GRT_MODE_IMAGE or GRT_MODE_DISK"},
         {p->integrator == GRT_RK4 || p->integrator == GRT_RK45, "grt_params.integrator: GRT_RK4 or GRT_RK45"},
-        {p->precision == GRT_PREC_FP64 || p->precision == GRT_PREC_MIXED,
-         "grt_params.precision: GRT_PREC_FP64 or GRT_PREC_MIXED"},
+        {p->precision == GRT_PREC_FP64 || p->precision == GRT_PREC_MIXED || p->precision == GRT_PREC_MIXED_GRID,
+         "grt_params.precision: GRT_PREC_FP64, GRT_PREC_MIXED or GRT_PREC_MIXED_GRID"},
         {gen_ok, "grt_params.generator: GRT_GEN_BLACKBODY, GRT_GEN_POWER_LAW or GRT_GEN_CUSTOM"},
         {finite_positive(p->mass), "grt_params.mass: finite and positive"},
         {std::isfinite(p->spin) && std::fabs(p->spin) <= p->mass,

@@ -19,7 +19,7 @@ MODE_IMAGE, MODE_DISK = 0, 1
 RK4, RK45 = 0, 1
 GEN_BLACKBODY, GEN_POWER_LAW, GEN_CUSTOM = 0, 1, 2
 PHASE_DISK, PHASE_BACKWARD, PHASE_FORWARD, PHASE_ARRIVED, PHASE_REJECTED = 0, 1, 2, 3, 4
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_MIXED_GRID = 0, 1, 2
 
 _D, _I32, _I64, _U64 = C.c_double, C.c_int32, C.c_int64, C.c_uint64
 

@@ -50,8 +50,11 @@ enum { GRT_GEN_BLACKBODY = 0, GRT_GEN_POWER_LAW = 1, GRT_GEN_CUSTOM = 2 };
 enum { GRT_PHASE_DISK = 0, GRT_PHASE_IMAGE_BACKWARD = 1, GRT_PHASE_IMAGE_FORWARD = 2,
        GRT_PHASE_IMAGE_ARRIVED = 3, GRT_PHASE_REJECTED = 4 };
 /* Arithmetic form of the trace kernel. */
-enum { GRT_PREC_FP64 = 0,   /* all-FP64, operation order of the reference (parity form) */
-       GRT_PREC_MIXED = 1   /* FP32 stage/metric arithmetic, FP64 state + controller */ };
+enum { GRT_PREC_FP64 = 0,        /* all-FP64, operation order of the reference (parity form) */
+       GRT_PREC_MIXED = 1,       /* FP32 right-hand side after emission outside the fluid grid (and in RK4
+                                    steps); FP64 state, stage sums and controller */
+       GRT_PREC_MIXED_GRID = 2   /* as GRT_PREC_MIXED, and the FP32 right-hand side after emission inside
+                                    the grid too (r > 4M, away from the polar axis) */ };
 
 /*
  * Every runtime parameter the reference's step functor and step loop read.

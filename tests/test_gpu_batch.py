@@ -159,9 +159,15 @@ def test_batch_rejects_bad_specs(gpu):
         ctx.close()
 
 
-def test_mixed_precision_batch_error(gpu):
+@pytest.mark.parametrize("prec,bar", [(abi.PREC_MIXED, 1e-5), (abi.PREC_MIXED_GRID, 1e-3)],
+                         ids=["mixed", "mixed_grid"])
+def test_mixed_precision_batch_error(gpu, prec, bar):
     # each frequency channel of the C2 image (at 64x64 on a 64x32x32 grid) in
-    # the mixed form against the FP64 form: L2 relative Stokes-I error <= 1e-5
+    # a mixed form against the FP64 form, L2 relative Stokes-I error: the
+    # benchmark's 1e-5 bar for GRT_PREC_MIXED (FP32 only where the Stokes
+    # vector no longer changes); GRT_PREC_MIXED_GRID, which also runs FP32
+    # through the fluid after emission, is held to 1e-3 here and to the 1e-5
+    # bar by the benchmark before it can be the headline form
     base = mini(workloads.C2, 64, (64, 32, 32))
     bw = workloads.BatchWorkload("c2_small_x4freq", base,
                                  [(base.inclination_deg, base.pixels, f) for f in workloads.FREQ_CHANNELS_GHZ])
@@ -170,12 +176,13 @@ def test_mixed_precision_batch_error(gpu):
     specs = bw.specs(p)
     _, ref, _ = run_batch(gpu, p, grid, specs)
     pm = p.copy()
-    pm.precision = abi.PREC_MIXED
+    pm.precision = prec
     _, got, _ = run_batch(gpu, pm, grid, specs)
     for k in range(len(specs)):
         assert ref[k].image_I.any()
         err = stokes_l2_rel(got[k].image_I, ref[k].image_I)
-        assert err <= 1e-5, (k, err)
+        print(f"precision {prec} channel {k}: Stokes-I L2 relative error {err:.3g}")
+        assert err <= bar, (k, err)
 
 
 def channel_specs(p):
