@@ -307,6 +307,15 @@ GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, int need_k1
     for (int c = 0; c < 7; ++c) kk.at(5, c) = s[sidx(c)];
     double err = 0.0;
     bool finite = isfinite(s[4]);
+    // The norm is max_c RN(n_c / sc_c).  Rounding is monotone, so it equals
+    // RN(n_m / sc_m) for the component m of largest exact ratio, found by
+    // comparing exact cross products n_c sc_m against n_m sc_c (the product
+    // and its fma residual).  One division then replaces seven serial ones.
+    // That needs every x4, x5 finite and n_c, sc_c inside [2^-400, 2^400]
+    // (or n_c = 0), so that no product under- or overflows; otherwise the
+    // ratios are formed one by one as before.  n_c and sc_c go to slots 2
+    // and 3 (k3, k4: not read again in this attempt).
+    bool boxed = true;
 #pragma unroll 1
     for (int c = 0; c < 7; ++c) {
         const double si = kk.at(5, c);
@@ -314,10 +323,32 @@ GRT_DEV int rk45_attempt(const KParams& kp, double s[8], double* dl, int need_k1
         const double x4 = si + dt * (b41 * k1 + b43 * k3 + b44 * k4 + b45 * k5);
         const double x5 = si + dt * (b51 * k1 + b53 * k3 + b54 * k4 + b55 * k5 + b56 * k6);
         const double sc = kp.atol + kp.rtol * fmax(fabs(x5), fabs(x4));
-        const double ratio = fabs(x5 - x4) / sc;
-        if (!isfinite(x5) || !isfinite(ratio)) finite = false;
-        err = fmax(err, ratio);
+        const double n = fabs(x5 - x4);
+        boxed = boxed && isfinite(x4) && isfinite(x5) && div_within<-400, 399>(sc) &&
+                div_zero_or_within<-400, 399>(n);
         kk.at(5, c) = x5;
+        kk.at(2, c) = n;
+        kk.at(3, c) = sc;
+    }
+    if (boxed) {
+        double nm = kk.at(2, 0), sm = kk.at(3, 0);
+#pragma unroll 1
+        for (int c = 1; c < 7; ++c) {
+            const double n = kk.at(2, c), sc = kk.at(3, c);
+            const double p = n * sm, q = nm * sc;
+            if (p > q || (p == q && fma(n, sm, -p) > fma(nm, sc, -q))) {
+                nm = n;
+                sm = sc;
+            }
+        }
+        err = div_by(nm, sm, div_recip(sm));
+    } else {
+#pragma unroll 1
+        for (int c = 0; c < 7; ++c) {
+            const double ratio = kk.at(2, c) / kk.at(3, c);
+            if (!isfinite(kk.at(5, c)) || !isfinite(ratio)) finite = false;
+            err = fmax(err, ratio);
+        }
     }
     if (!finite) {
         *dl = dt * kp.min_scale;
