@@ -16,6 +16,7 @@
 #include <math.h>
 
 #include "grt_div.cuh"
+#include "grt_rn.cuh"
 
 namespace grt {
 namespace dev {
@@ -119,6 +120,23 @@ GRT_DEV Rhs7 ks_rhs(double x, double y, double z, double pt, double px, double p
 // divided by at most r^8 <= 2^160.  Outside it `ok` is false and the caller
 // evaluates ks_rhs.  The expression tree is ks_rhs's, so the result equals
 // ks_rhs bit for bit.
+// BF selects the branch-free reciprocal and square root of grt_rn.cuh (equal
+// to __drcp_rn and sqrt on every argument that reaches them here: the square
+// roots' results are checked against the box before use, and every
+// reciprocal's argument lies in [2^-192, 2^164]); without it, CUDA's.
+template <bool BF>
+GRT_DEV double rhs_recip(double b) {
+    if constexpr (BF) return rcp_rn_box(b);
+    else return div_recip(b);
+}
+
+template <bool BF>
+GRT_DEV double rhs_sqrt(double v) {
+    if constexpr (BF) return sqrt_rn_box(v);
+    else return sqrt(v);
+}
+
+template <bool BF = false>
 GRT_DEV Rhs7 ks_rhs_rcp(double x, double y, double z, double pt, double px, double py, double pz,
                         double a, double M, bool& ok) {
     const double rsq = x * x + y * y + z * z;
@@ -126,24 +144,24 @@ GRT_DEV Rhs7 ks_rhs_rcp(double x, double y, double z, double pt, double px, doub
     // Two square-root sites (unlike ks_radius): the reciprocal of S and the
     // quotients that use it then overlap the second square root, which
     // measured 3% faster on a lane-per-SM workload than one rolled site.
-    const double S = sqrt(A * A + 4.0 * ((a * z) * (a * z)));
-    const double r = sqrt(0.5 * (A + S));
+    const double S = rhs_sqrt<BF>(A * A + 4.0 * ((a * z) * (a * z)));
+    const double r = rhs_sqrt<BF>(0.5 * (A + S));
     ok = div_zero_or_within<-20, 19>(x) && div_zero_or_within<-20, 19>(y) && div_zero_or_within<-20, 19>(z) &&
          div_within<-24, 19>(r) && div_within<-60, 41>(S);
     Rhs7 o{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (!ok) return o;
-    const double yS = div_recip(S);
+    const double yS = rhs_recip<BF>(S);
     const double opas = 1.0 + div_by(A, S, yS);
     const double two_r = 2.0 * r;
     // RN(1/(2r)) = RN(1/r) / 2 exactly: r is inside the box, so no rounding
     // step under- or overflows
-    const double yr = div_recip(r);
+    const double yr = rhs_recip<BF>(r);
     const double y2r = 0.5 * yr;
     const double dr0 = div_by(x * opas, two_r, y2r);
     const double dr1 = div_by(y * opas, two_r, y2r);
     const double dr2 = div_by(z * opas + div_by(2.0 * (a * a) * z, S, yS), two_r, y2r);
     const double B = r * r + a * a;
-    const double yB = div_recip(B);
+    const double yB = rhs_recip<BF>(B);
     const double l1 = div_by(r * x + a * y, B, yB);
     const double l2 = div_by(r * y - a * x, B, yB);
     const double l3 = div_by(z, r, yr);
@@ -162,7 +180,7 @@ GRT_DEV Rhs7 ks_rhs_rcp(double x, double y, double z, double pt, double px, doub
     const double r2 = r * r;
     const double r3 = r2 * r;
     const double D = r3 * r + (a * z) * (a * z);
-    const double yD = div_recip(D);
+    const double yD = rhs_recip<BF>(D);
     const double H = div_by(M * r3, D, yD);
     const double four_r3 = 4.0 * r3;
     const double dD0 = four_r3 * dr0;
@@ -170,7 +188,7 @@ GRT_DEV Rhs7 ks_rhs_rcp(double x, double y, double z, double pt, double px, doub
     const double dD2 = four_r3 * dr2 + 2.0 * (a * a) * z;
     const double three_r2 = 3.0 * r2;
     const double DD = D * D;
-    const double yDD = div_recip(DD);
+    const double yDD = rhs_recip<BF>(DD);
     const double dH0 = div_by(M * (three_r2 * dr0 * D - r3 * dD0), DD, yDD);
     const double dH1 = div_by(M * (three_r2 * dr1 * D - r3 * dD1), DD, yDD);
     const double dH2 = div_by(M * (three_r2 * dr2 * D - r3 * dD2), DD, yDD);

@@ -38,13 +38,15 @@
 namespace grt {
 namespace dev {
 
-struct MixedRhs {
+// BF: the FP64 part is Fp64RhsT<BF>.
+template <bool BF>
+struct MixedRhsT {
     static GRT_DEV V7 eval(const double s[8], const KParams& kp, int fast) {
         const double x = s[1], y = s[2], z = s[3];
         const double rho2 = x * x + y * y;
         const double rsq = rho2 + z * z;
         if (!fast || rsq < kp.fp64_radius_sq || rho2 < kp.fp64_axis_sin2 * rsq)
-            return Fp64Rhs::eval(s, kp, 0);
+            return Fp64RhsT<BF>::eval(s, kp, 0);
         return to_v7(ks_rhs_fp32(x, y, z, rsq, s[4], s[5], s[6], s[7], kp.a, kp.M));
     }
 
@@ -73,6 +75,7 @@ struct MixedRhs {
         s[7] = alpha * pz;
     }
 };
+using MixedRhs = MixedRhsT<false>;
 
 }  // namespace dev
 }  // namespace grt

@@ -59,19 +59,24 @@ static __device__ __noinline__ Rhs7 ks_rhs_ieee(double x, double y, double z, do
 
 // Right-hand-side policy of the FP64 parity form: ks_rhs_rcp (reciprocal
 // quotients that round like IEEE divisions) inside its box, ks_rhs outside;
-// both give ks_rhs's result bit for bit.
+// both give ks_rhs's result bit for bit.  BF: ks_rhs_rcp with the branch-free
+// reciprocal and square root (grt_rn.cuh), which a lone warp per scheduler
+// runs faster (C1's 4,096 rays: 3% on the trace) and the disk-mode kernel,
+// at 170 registers, slower (2%); the image-mode kernels use it.
 // `fast` is the per-call precision hint of the mixed form (ignored here).
-struct Fp64Rhs {
+template <bool BF>
+struct Fp64RhsT {
     static GRT_DEV V7 eval(const double s[8], const KParams& kp, int /*fast*/) {
         if (kp.rcp_ok) {
             bool ok;
-            const Rhs7 o = ks_rhs_rcp(s[1], s[2], s[3], s[4], s[5], s[6], s[7], kp.a, kp.M, ok);
+            const Rhs7 o = ks_rhs_rcp<BF>(s[1], s[2], s[3], s[4], s[5], s[6], s[7], kp.a, kp.M, ok);
             if (ok) return to_v7(o);
         }
         return to_v7(ks_rhs_ieee(s[1], s[2], s[3], s[4], s[5], s[6], s[7], kp.a, kp.M));
     }
     static GRT_DEV void after_accept(double*, const KParams&, int) {}
 };
+using Fp64Rhs = Fp64RhsT<false>;
 
 struct Lane {
     double s[8];

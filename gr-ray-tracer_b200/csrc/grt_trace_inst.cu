@@ -12,13 +12,17 @@
 #include "grt_launch.h"
 #include "grt_trace.cuh"
 
+// The image-mode legs take the branch-free reciprocal and square root in the
+// FP64 right-hand side (dev::Fp64RhsT<true>); the disk-mode kernel measured
+// slower with them and keeps CUDA's.
+#define GRT_RHS_BF (GRT_LEG != 3)
 #if GRT_MIXED
 #include "grt_rhs_mixed.cuh"
 #define GRT_TRACE_KERNEL trace_mixed
-#define GRT_TRACE_RHS dev::MixedRhs
+#define GRT_TRACE_RHS dev::MixedRhsT<GRT_RHS_BF>
 #else
 #define GRT_TRACE_KERNEL trace_fp64
-#define GRT_TRACE_RHS dev::Fp64Rhs
+#define GRT_TRACE_RHS dev::Fp64RhsT<GRT_RHS_BF>
 #endif
 #define GRT_CAT2(a, b) a##b
 #define GRT_CAT(a, b) GRT_CAT2(a, b)

@@ -15,7 +15,13 @@ the trace kernels):
   magnitude below 2^-20 or above 2^20) must be reported outside;
 * the RK45 controller's pow_quarter on the device against this host's glibc
   pow(x, 0.25), bit for bit, on tie-near inputs (tests/golden/pow_quarter_hard.npz)
-  and on random inputs over the controller's range and over all doubles."""
+  and on random inputs over the controller's range and over all doubles;
+* the branch-free reciprocal and square root of the image-mode kernels
+  (grt_rn.cuh) against CUDA's __drcp_rn and sqrt, bit for bit, on random
+  arguments over their exact ranges ([2^-1000, 2^1000] for the reciprocal,
+  [2^-900, 2^1000] for the square root), significands near all ones and near one,
+  and arguments next to squares of rounding midpoints; and ks_rhs_rcp with
+  them against ks_rhs_rcp with CUDA's, components and box flag."""
 
 import ctypes as C
 from pathlib import Path
@@ -38,6 +44,8 @@ def selftest(gpu):
     L.grt_selftest_division.argtypes = [_DP, _DP, C.c_size_t, _DP, _DP]
     L.grt_selftest_rhs.argtypes = [_DP, C.c_size_t, C.c_double, C.c_double, _DP, _DP, _UP]
     L.grt_selftest_pow_quarter.argtypes = [_DP, C.c_size_t, _DP]
+    L.grt_selftest_rn_box.argtypes = [_DP, C.c_size_t, _DP, _DP, _DP, _DP]
+    L.grt_selftest_rhs_bf.argtypes = [_DP, C.c_size_t, C.c_double, C.c_double, _DP, _DP, _UP]
     return L
 
 
@@ -167,3 +175,77 @@ def test_device_pow_quarter_is_glibc_pow(selftest, oracle):
     assert_bitwise(y, want)
     assert_bitwise(host, want)
     assert np.array_equal(y[: g["x_controller"].size], g["pow_controller"])
+
+
+def rn_box(L, x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = [np.empty(x.size) for _ in range(4)]
+    assert L.grt_selftest_rn_box(dp(x), x.size, *(dp(o) for o in out)) == 0
+    return out
+
+
+def test_branch_free_reciprocal_and_sqrt_are_cudas(selftest):
+    rng = np.random.default_rng(19)
+    n = 1 << 22
+    e = rng.integers(-1000, 1000, n)
+    sign = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+    random = sign * np.ldexp(1.0 + rng.integers(0, 1 << 52, n, dtype=np.int64) * 2.0 ** -52, e)
+    k = rng.integers(0, 1 << 16, n)
+    near_two = sign * np.ldexp(2.0 - k * 2.0 ** -52, e)     # all ones at k = 1
+    near_one = sign * np.ldexp(1.0 + k * 2.0 ** -52, e)
+    ones = np.ldexp(2.0 - 2.0 ** -52, np.arange(-999, 1000))  # every all-ones significand's exponent
+    edges = np.array([2.0 ** -1000, 2.0 ** -900, 2.0 ** 1000, 1.0, 2.0, 3.0, 0.5, 1.0 + 2.0 ** -52,
+                      2.0 - 2.0 ** -51])
+    for x in (random, near_two, near_one, np.concatenate([ones, -ones, edges, -edges])):
+        rb, rc, sb, sc = rn_box(selftest, x)
+        assert_bitwise(rb, rc)
+        assert_bitwise(sb, sc, np.abs(x) >= 2.0 ** -900)
+    # next to squares of midpoints: sqrt lies within a tiny fraction of an
+    # ulp of a rounding boundary
+    m = np.ldexp(1.0 + rng.integers(0, 1 << 52, n // 8, dtype=np.int64) * 2.0 ** -52, rng.integers(-449, 490, n // 8))
+    ulp = np.nextafter(m, np.inf) - m
+    v = m * m + m * ulp
+    for d in range(-3, 4):
+        w = v.view(np.int64) + d
+        _, _, sb, sc = rn_box(selftest, w.view(np.float64))
+        assert_bitwise(sb, sc)
+
+
+def test_branch_free_outside_arguments_fail_the_box(selftest):
+    # zero, subnormal, infinity and NaN give NaN from the square root, which
+    # fails ks_rhs_rcp's box check as CUDA's out-of-box results do; below
+    # 2^-900 the result stays below 2^-450, far outside the box
+    x = np.array([0.0, 5e-324, 2.0 ** -1060, np.inf, np.nan])
+    _, _, sb, _ = rn_box(selftest, x)
+    assert np.isnan(sb).all(), sb
+    rng = np.random.default_rng(29)
+    low = np.ldexp(1.0 + rng.random(1 << 16), rng.integers(-1022, -900, 1 << 16))
+    _, _, sb, sc = rn_box(selftest, low)
+    assert (sb < 2.0 ** -449).all() and (np.abs(sb - sc) <= np.spacing(sc)).all()
+
+
+def rhs_bf(L, s, spin, M=1.0):
+    n = s.shape[0]
+    bf, ref = np.empty((n, 7)), np.empty((n, 7))
+    inside = np.empty(n, dtype=np.uint32)
+    assert L.grt_selftest_rhs_bf(dp(s), n, spin, M, dp(bf), dp(ref), inside.ctypes.data_as(_UP)) == 0
+    return bf, ref, inside
+
+
+@pytest.mark.parametrize("spin", [0.0, 0.94, 1.0, -0.7])
+def test_branch_free_rhs_is_the_rhs(selftest, spin):
+    rng = np.random.default_rng(int(abs(spin) * 1000) + 23)
+    s = random_states(rng, 1 << 19, spin)
+    out = np.tile(np.array([[10.0, -20.0, 5.0, -1.0, 0.3, -0.5, 0.8]]), (5, 1))
+    out[0, 0] = 2.0 ** -21
+    out[1, 1] = -(2.0 ** 21)
+    out[2, 2] = np.nan
+    out[3, 0] = 5e-324
+    out[4, :3] = [spin, 0.0, 0.0]   # on the ring: S = 0
+    s = np.ascontiguousarray(np.vstack([s, out]))
+    bf, ref, inside = rhs_bf(selftest, s, spin)
+    ok_bf, ok_ref = (inside & 1).astype(bool), (inside & 2).astype(bool)
+    assert np.array_equal(ok_bf, ok_ref)
+    assert ok_bf.mean() > 0.99
+    assert not ok_bf[-5:].any()
+    assert_bitwise(bf.ravel(), ref.ravel(), np.repeat(ok_ref, 7))
