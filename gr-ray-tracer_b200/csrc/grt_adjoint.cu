@@ -55,7 +55,9 @@ GRT_DEV void load_checkpoint(const double* c, Lane& L) {
 
 // One call of the reference functor on this ray (the trace kernels' per-call
 // sequence: termination radii, RK4 step or up to 12 RKF45 attempts, post_step).
-// Returns 1 if the photon terminated.
+// Returns 1 if the photon terminated.  The right-hand side takes the
+// branch-free reciprocal and square root (Fp64RhsT<true>): with one ray per
+// thread and about one warp per scheduler, both passes measured 5% faster.
 template <int INTEGRATOR, class Rec>
 GRT_DEV int run_call(const KParams& kp, const Axes& ax, const KStore& kk, Lane& L, double& tdisp, double& pdisp,
                      int& have_disp, Rec rec) {
@@ -74,13 +76,13 @@ GRT_DEV int run_call(const KParams& kp, const Axes& ax, const KStore& kk, Lane& 
     if (INTEGRATOR == 0) {
         const int phase0 = L.phase;
         const double taken = L.dl;
-        rk4_step<Fp64Rhs>(L.s, taken, kp, 1);
+        rk4_step<Fp64RhsT<true>>(L.s, taken, kp, 1);
         return post_step<false, Rec>(kp, ax, L, phase0, taken, step, tdisp, pdisp, have_disp, rec);
     }
     L.dl_try = L.dl;
     for (int attempt = 0; attempt < 12; ++attempt) {
         const double taken = L.dl_try;
-        if (rk45_attempt<Fp64Rhs>(kp, L.s, &L.dl_try, attempt == 0, 0, kk)) {
+        if (rk45_attempt<Fp64RhsT<true>>(kp, L.s, &L.dl_try, attempt == 0, 0, kk)) {
             L.dl = L.dl_try;
             const int phase0 = L.phase;
             return post_step<false, Rec>(kp, ax, L, phase0, taken, step, tdisp, pdisp, have_disp, rec);
