@@ -46,6 +46,27 @@ GRT_DEV double ks_radius(double x, double y, double z, double a) {
     return r;
 }
 
+// ks_radius out of line: the fallback of ks_radius_bf.
+static __device__ __noinline__ double ks_radius_ieee(double x, double y, double z, double a) {
+    return ks_radius(x, y, z, a);
+}
+
+// ks_radius with the branch-free square root (grt_rn.cuh) when both of its
+// arguments lie in that function's exact range, [2^-900, 2^1000]; otherwise
+// ks_radius itself.  The same value as ks_radius for every input: the test
+// comes after both square roots, so they overlap with the work around them
+// instead of waiting behind sqrt's slow-path branch.
+GRT_DEV double ks_radius_bf(double x, double y, double z, double a) {
+    const double rsq = x * x + y * y + z * z;
+    const double A = rsq - a * a;
+    const double v1 = A * A + 4.0 * ((a * z) * (a * z));
+    const double S = sqrt_rn_box(v1);
+    const double v2 = 0.5 * (A + S);
+    const double r = sqrt_rn_box(v2);
+    if (div_within<-900, 999>(v1) && div_within<-900, 999>(v2)) return r;
+    return ks_radius_ieee(x, y, z, a);
+}
+
 // kerr_schild_core.hpp:157-192 (with compute_r_and_deriv :36-46,
 // compute_l_and_deriv :58-77, compute_H_and_deriv :85-95 inlined).
 GRT_DEV Rhs7 ks_rhs(double x, double y, double z, double pt, double px, double py, double pz,

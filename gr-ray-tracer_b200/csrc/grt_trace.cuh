@@ -63,9 +63,15 @@ static __device__ __noinline__ Rhs7 ks_rhs_ieee(double x, double y, double z, do
 // reciprocal and square root (grt_rn.cuh), which a lone warp per scheduler
 // runs faster (C1's 4,096 rays: 3% on the trace) and the disk-mode kernel,
 // at 170 registers, slower (2%); the image-mode kernels use it.
+// LAT: the instantiation is latency-bound (one warp or so per scheduler: the
+// 2-blocks/SM kernels), where the mixed form's renormalisation with the
+// branch-free functions and the branch-free Kerr-Schild radius (ks_radius_bf)
+// measured 4.6% faster on C1; at 4 blocks/SM and 128 registers the radius
+// measured 1% slower, so the others keep ks_radius.
 // `fast` is the per-call precision hint of the mixed form (ignored here).
-template <bool BF>
+template <bool BF, bool LAT = false>
 struct Fp64RhsT {
+    static constexpr bool kLatency = LAT;
     static GRT_DEV V7 eval(const double s[8], const KParams& kp, int /*fast*/) {
         if (kp.rcp_ok) {
             bool ok;
@@ -74,7 +80,8 @@ struct Fp64RhsT {
         }
         return to_v7(ks_rhs_ieee(s[1], s[2], s[3], s[4], s[5], s[6], s[7], kp.a, kp.M));
     }
-    static GRT_DEV void after_accept(double*, const KParams&, int) {}
+    // nothing to do after an accepted step; no radius computed (-1)
+    static GRT_DEV double after_accept(double*, const KParams&, int) { return -1.0; }
 };
 using Fp64Rhs = Fp64RhsT<false>;
 
@@ -510,11 +517,16 @@ GRT_DEV int generate_at_contact(const KParams& kp, Lane& L, const FluidSample& f
 // channels that terminated on their own in this call.
 // LEG (see trace_body) removes the code the leg never runs: generation from
 // the forward leg, transfer and the camera from the backward leg.
-template <bool RAW = false, class Rec = NoRecord, bool SHARE = false, int LEG = 0>
+// radius_hint: the Kerr-Schild radius of L.s when the caller already has it
+// (the mixed form's renormalisation computes it), else negative.  FASTR: the
+// radius through ks_radius_bf (latency-bound instantiations).
+template <bool RAW = false, class Rec = NoRecord, bool SHARE = false, int LEG = 0, bool FASTR = false>
 GRT_DEV int post_step(const KParams& kp, const Axes& ax, Lane& L, int phase0, double taken, int64_t step,
-                      double& tdisp, double& pdisp, int& have_disp, Rec rec = Rec(), int* ch_term = nullptr) {
+                      double& tdisp, double& pdisp, int& have_disp, Rec rec = Rec(), int* ch_term = nullptr,
+                      double radius_hint = -1.0) {
     const KImage& im = image_params(kp, L.img);
-    L.radius = ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
+    if (radius_hint >= 0.0) L.radius = radius_hint;
+    else L.radius = FASTR ? ks_radius_bf(L.s[1], L.s[2], L.s[3], kp.a) : ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
     L.have_radius = 1;
     const bool backward = phase0 == 1;  // ImageBackward
     // LEG 3 (disk mode) compiles the image-mode branches out of the step loop
@@ -752,7 +764,9 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
             } else {
                 ++L.calls;
                 ++cnt.calls;
-                const double r = L.have_radius ? L.radius : ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
+                const double r = L.have_radius   ? L.radius
+                                 : RHS::kLatency ? ks_radius_bf(L.s[1], L.s[2], L.s[3], kp.a)
+                                                 : ks_radius(L.s[1], L.s[2], L.s[3], kp.a);
                 if (r <= kp.r_min) {
                     L.I[0] = L.I[1] = L.I[2] = L.I[3] = 0.0;
                     L.zero_all = 1;
@@ -765,12 +779,12 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                     const int phase0 = L.phase;
                     const double taken = L.dl;
                     rk4_step<RHS>(L.s, taken, kp, 1);
-                    RHS::after_accept(L.s, kp, 1);
+                    const double rn = RHS::after_accept(L.s, kp, 1);
                     ++cnt.accepted;
                     int ch_term = 0;
-                    terminated = post_step<RAW, NoRecord, SHARE, LEG>(kp, ax, L, phase0, taken,
-                                                                      kp.step0 + L.calls - 1, tdisp, pdisp, have_disp,
-                                                                      NoRecord(), &ch_term);
+                    terminated = post_step<RAW, NoRecord, SHARE, LEG, RHS::kLatency>(
+                        kp, ax, L, phase0, taken, kp.step0 + L.calls - 1, tdisp, pdisp, have_disp, NoRecord(), &ch_term,
+                        rn);
                     if (SHARE && ch_term) {
                         cnt.terminated += ch_term;
                         const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);
@@ -798,14 +812,14 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
             L.need_k1 = 0;
             ++L.attempts;
             if (ok) {
-                RHS::after_accept(L.s, kp, L.fast);
+                const double rn = RHS::after_accept(L.s, kp, L.fast);
                 ++cnt.accepted;
                 L.dl = L.dl_try;
                 L.mid_call = 0;
                 const int phase0 = L.phase;
                 int ch_term = 0;
-                terminated = post_step<RAW, NoRecord, SHARE, LEG>(kp, ax, L, phase0, taken, kp.step0 + L.calls - 1,
-                                                                  tdisp, pdisp, have_disp, NoRecord(), &ch_term);
+                terminated = post_step<RAW, NoRecord, SHARE, LEG, RHS::kLatency>(
+                    kp, ax, L, phase0, taken, kp.step0 + L.calls - 1, tdisp, pdisp, have_disp, NoRecord(), &ch_term, rn);
                 if (SHARE && ch_term) {
                     cnt.terminated += ch_term;
                     const unsigned long long ts = static_cast<unsigned long long>(kp.step0 + L.calls);

@@ -16,13 +16,15 @@
 // FP64 right-hand side (dev::Fp64RhsT<true>); the disk-mode kernel measured
 // slower with them and keeps CUDA's.
 #define GRT_RHS_BF (GRT_LEG != 3)
+// The 2-blocks/SM kernels (255 registers; the workloads with about one warp
+// per scheduler) are latency-bound: their policies take LAT (grt_trace.cuh).
 #if GRT_MIXED
 #include "grt_rhs_mixed.cuh"
 #define GRT_TRACE_KERNEL trace_mixed
-#define GRT_TRACE_RHS dev::MixedRhsT<GRT_RHS_BF>
+#define GRT_TRACE_RHS(MINB) dev::MixedRhsT<GRT_RHS_BF, (MINB) == 2>
 #else
 #define GRT_TRACE_KERNEL trace_fp64
-#define GRT_TRACE_RHS dev::Fp64RhsT<GRT_RHS_BF>
+#define GRT_TRACE_RHS(MINB) dev::Fp64RhsT<GRT_RHS_BF, (MINB) == 2>
 #endif
 #define GRT_CAT2(a, b) a##b
 #define GRT_CAT(a, b) GRT_CAT2(a, b)
@@ -36,7 +38,7 @@ __global__ void __launch_bounds__(128, MINB) GRT_TRACE_KERNEL(const __grid_const
     dev::Axes ax;
     dev::KStore kk;
     dev::stage_grid(kp, smem, INTEGRATOR, ax, kk);
-    dev::trace_body<INTEGRATOR, GRT_TRACE_RHS, false, SHARE, LEG>(kp, ax, kk);
+    dev::trace_body<INTEGRATOR, GRT_TRACE_RHS(MINB), false, SHARE, LEG>(kp, ax, kk);
 }
 
 namespace {
