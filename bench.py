@@ -31,10 +31,17 @@ another on one context).  L2 is flushed (a 256 MB device write) before every
 timed step: outside the events for the forms and the serial e2e, on the
 stream inside the timed region for the streamed e2e.
 
+On one GPU the default run then measures the other configurations, each by
+this script in a child process of its own after the headline's timed region
+(C1 64x64 RK4; C3 the 64-image batch; C4 the adjoint; C5 disk mode), and
+reports a summary of each under `other_workloads` in the same line
+(--no-other-workloads skips them; --workload c1/c3/c4/c5 runs one alone).
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank traces its own full batch (replicas, weak scaling);
-times are CUDA-event times, max over ranks.
+Under torchrun each rank renders one frame of a camera orbit (camera_phi =
+2 pi k / N) and the image products are all-gathered over NCCL every step
+(weak scaling); times are CUDA-event times, max over ranks.
 """
 
 from __future__ import annotations
@@ -44,6 +51,7 @@ import json
 import math
 import os
 import statistics
+import subprocess
 import sys
 import tempfile
 import time
@@ -601,10 +609,54 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "clocks": clocks,
         }
+        if world == 1 and args.workload == "c2" and not args.no_other_workloads:
+            line["other_workloads"] = other_workloads()
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# The other configurations: workload and timed steps of each.
+OTHER_WORKLOADS = (("c1", 10), ("c3", 3), ("c4", 10), ("c5", 2))
+
+
+def other_workloads():
+    """C1, C3, C4 and C5, each run by this script in a child process of its own
+    (its own timing rules: warm-up, L2 flush, CUDA events) after the headline's
+    timed region has ended, so that one default run reports every
+    configuration.  Each entry is a summary of that run's JSON line, or the
+    reason it failed."""
+    out = {}
+    for wl, steps in OTHER_WORKLOADS:
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", wl, "--steps", str(steps), "--warmup", "3",
+               "--no-cpu-baseline"]
+        env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE")}
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900, env=env)
+            lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+            if r.returncode != 0 or not lines:
+                out[wl] = {"error": f"exit {r.returncode}: {r.stderr.strip()[-300:]}"}
+                continue
+            d = json.loads(lines[-1])
+        except Exception as e:  # a failed configuration must not cost the headline line
+            out[wl] = {"error": repr(e)[:300]}
+            continue
+        keys = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "dtype", "gpu_launches", "forward_ms",
+                "adjoint_ms", "emission_ms", "transport_ms", "rk_steps_per_s", "geodesics_per_s", "packets")
+        summary = {k: d[k] for k in keys if k in d}
+        summary["workload"] = (d.get("config") or {}).get("workload")
+        if d.get("roofline"):
+            summary["roofline_frac"] = d["roofline"].get("frac")
+        if isinstance(d.get("e2e"), dict):
+            summary["e2e"] = d["e2e"].get("value")
+        if d.get("forms"):
+            summary["forms"] = {k: {"rays_per_s": v.get("rays_per_s"), "trace_ms_per_launch": v.get("trace_ms_per_launch")}
+                                for k, v in d["forms"].items()}
+        if d.get("clocks"):
+            summary["clocks"] = {k: d["clocks"].get(k) for k in ("sm_mhz", "reasons")}
+        out[wl] = summary
+    return out
 
 
 def cpu_baseline(w, reps=2, params=None, label=None):
@@ -821,6 +873,8 @@ def main():
     ap.add_argument("--workload", default="c2", choices=("c1", "c2", "c3", "c4", "c5"),
                     help="c2 (the headline), c1, c3 (the 64-image batch), c4 (adjoint), c5 (disk mode)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-workloads", action="store_true",
+                    help="c2 on one GPU: skip the runs of c1, c3, c4 and c5 that follow the headline")
     ap.add_argument("--no-autotune", action="store_true", help="use the library's default launch shape")
     ap.add_argument("--forms", default="fp64,fp64_batched,mixed_batched",
                     help="comma list of fp64, fp64_batched, mixed_batched, mixed_grid_batched")
