@@ -174,6 +174,10 @@ struct grt_ctx {
     bool groups_share = false;            // some group has two or more channels
     unsigned long long geodesics = 0;     // queue length with sharing
     DevBuf<unsigned long long> group_qstart_dev;
+    // tile orders of the image-mode queue (queue position -> index): over
+    // photon slots and over the geodesics of channel groups
+    DevBuf<unsigned> order_ph, order_geo;
+    bool order_ph_ok = false, order_geo_ok = false;
     DevBuf<int> group_chan_dev, chan_img_dev;
     DevBuf<unsigned long long> share_state;  // [geodesics] lead / finished channels (KParams::share_state)
     DevBuf<long long> calls_carry;           // [queue] calls taken in the backward-leg launch
@@ -323,6 +327,9 @@ grt::KParams make_kparams(const grt_ctx* c) {
         k.n = c->geodesics;
         k.share_state = c->share_state.ptr;
     }
+    if (k.image_mode && c->have_images && !c->random_screen)
+        k.order = k.ngroups > 0 ? (c->order_geo_ok ? c->order_geo.ptr : nullptr)
+                                : (c->order_ph_ok ? c->order_ph.ptr : nullptr);
     k.calls_carry = c->calls_carry.ptr;
     k.counters = c->counters.ptr;
     k.refill_threshold = c->lc.refill_threshold;
@@ -404,6 +411,7 @@ void grt_destroy(grt_ctx* c) {
     c->image.release(); c->spectrum.release(); c->arrived.release(); c->scratch_u64.release();
     c->images_dev.release(); c->image_start_dev.release();
     c->group_qstart_dev.release(); c->group_chan_dev.release(); c->chan_img_dev.release();
+    c->order_ph.release(); c->order_geo.release();
     c->m_abs.release(); c->m_emis.release();
     c->ckpt.release(); c->tape.release(); c->dLdI.release(); c->g_abs.release(); c->g_emis.release();
     c->nckpt.release(); c->adj_overflow.release(); c->call0.release();
@@ -774,6 +782,49 @@ grt_status launch_image_inits(grt_ctx* c) {
     return GRT_OK;
 }
 
+// Appends the queue indices start .. start + nx ny - 1 of one row-major
+// nx x ny pixel block in tile order: 8 x 4 tiles, left to right, top to
+// bottom, each tile row by row (edge tiles are cut to the block).  A warp
+// that claims 32 consecutive queue positions then traces one tile.  Measured
+// on C2 (256 x 256, RK45): the trace 3.2% faster than with 32 x 1 row segments
+// (4 x 8 and 16 x 2 tiles gained less; ordering by screen radius lost 5%).
+void append_tile_order(std::vector<unsigned>& out, unsigned long long start, uint64_t nx, uint64_t ny) {
+    constexpr uint64_t kTw = 8, kTh = 4;
+    for (uint64_t ty = 0; ty < ny; ty += kTh)
+        for (uint64_t tx = 0; tx < nx; tx += kTw)
+            for (uint64_t y = ty; y < ty + kTh && y < ny; ++y)
+                for (uint64_t x = tx; x < tx + kTw && x < nx; ++x)
+                    out.push_back(static_cast<unsigned>(start + y * nx + x));
+}
+
+// Builds and uploads the tile orders of the image set just laid out.
+grt_status set_tile_orders(grt_ctx* c, const std::vector<unsigned long long>& start,
+                           const std::vector<unsigned long long>& qstart, const std::vector<int>& gchan,
+                           const std::vector<int>& chan) {
+    c->order_ph_ok = c->order_geo_ok = false;
+    if (c->random_screen || c->n >= (1ull << 32)) return GRT_OK;
+    std::vector<unsigned> ord;
+    ord.reserve(c->n);
+    for (size_t k = 0; k + 1 < start.size(); ++k)
+        append_tile_order(ord, start[k], c->images[k].nx, (start[k + 1] - start[k]) / c->images[k].nx);
+    GRT_CUDA(c, c->order_ph.alloc(ord.size()), "alloc queue order");
+    GRT_CUDA(c, cudaMemcpy(c->order_ph.ptr, ord.data(), ord.size() * sizeof(unsigned), cudaMemcpyHostToDevice),
+             "H2D queue order");
+    c->order_ph_ok = ord.size() == c->n;
+    if (!qstart.empty()) {
+        ord.clear();
+        for (size_t g = 0; g + 1 < qstart.size(); ++g) {
+            const grt_image_spec& lead = c->images[chan[gchan[g]]];
+            append_tile_order(ord, qstart[g], lead.nx, lead.ny);
+        }
+        GRT_CUDA(c, c->order_geo.alloc(ord.size()), "alloc queue order");
+        GRT_CUDA(c, cudaMemcpy(c->order_geo.ptr, ord.data(), ord.size() * sizeof(unsigned), cudaMemcpyHostToDevice),
+                 "H2D queue order");
+        c->order_geo_ok = ord.size() == c->geodesics;
+    }
+    return GRT_OK;
+}
+
 grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages, uint64_t id_offset, bool batched,
                          double forward_back = 0.0, uint64_t row0 = 0, uint64_t nrows = 0,
                          bool random_screen = false) {
@@ -861,9 +912,13 @@ grt_status set_image_set(grt_ctx* c, const grt_image_spec* specs, size_t nimages
                  "H2D groups");
         GRT_CUDA(c, cudaMemcpy(c->chan_img_dev.ptr, chan.data(), chan.size() * sizeof(int), cudaMemcpyHostToDevice),
                  "H2D groups");
+        const grt_status os = set_tile_orders(c, start, qstart, gchan, chan);
+        if (os != GRT_OK) return os;
     } else {
         c->ngroups = 0;
         c->groups_share = false;
+        const grt_status os = set_tile_orders(c, start, {}, {}, {});
+        if (os != GRT_OK) return os;
     }
     return launch_image_inits(c);
 }

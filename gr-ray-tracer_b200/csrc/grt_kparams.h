@@ -120,6 +120,9 @@ struct KParams {
     // geodesic as the last launch left it; zeroed with the photons' init
     // (nullptr: channel 0 leads and none finished)
     unsigned long long* share_state;
+    // image mode: queue position -> queue index, so that each warp's 32
+    // claims are an 8 x 4 tile of one image's pixels (nullptr = identity)
+    const unsigned* order;
     int refill_threshold;      // idle lanes before a warp refills (1..32)
     int grab;                  // photons claimed per queue access (per warp)
     const double* m_abs;       // optional per-cell multipliers on dtau (nullptr = 1)

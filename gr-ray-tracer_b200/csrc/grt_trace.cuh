@@ -714,6 +714,9 @@ GRT_DEV void trace_body(const KParams& kp, const Axes& ax, const KStore& kk) {
                     long long q = -1;
                     if (rank < take_a) q = static_cast<long long>(base_a + rank);
                     else if (rank - take_a < take_b) q = static_cast<long long>(base_b + (rank - take_a));
+                    // the queue hands out pixels in tiles (KParams::order); a
+                    // photon's calls do not depend on which lane takes it
+                    if (kp.order && q >= 0) q = static_cast<long long>(kp.order[q]);
                     long long slot = q;
                     if (SHARE && q >= 0) {
                         int lo = 0, hi = kp.ngroups - 1;
