@@ -177,6 +177,8 @@ struct grt_ctx {
     // tile orders of the image-mode queue (queue position -> index): over
     // photon slots and over the geodesics of channel groups
     DevBuf<unsigned> order_ph, order_geo;
+    // per-SM first-claim counters of the trace launches (KParams::sm_claims)
+    DevBuf<unsigned> sm_claims;
     bool order_ph_ok = false, order_geo_ok = false;
     DevBuf<int> group_chan_dev, chan_img_dev;
     DevBuf<unsigned long long> share_state;  // [geodesics] lead / finished channels (KParams::share_state)
@@ -381,7 +383,7 @@ grt_status grt_create(const grt_params* p, grt_ctx** out) {
     c->device = dev;
     c->sm_count = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        c->counters.alloc(1) != cudaSuccess || c->scratch_u64.alloc(4) != cudaSuccess ||
+        c->counters.alloc(1) != cudaSuccess || c->sm_claims.alloc(grt::kSmClaimSlots) != cudaSuccess || c->scratch_u64.alloc(4) != cudaSuccess ||
         cudaMallocHost(reinterpret_cast<void**>(&c->host_counters), sizeof(grt::KCounters)) != cudaSuccess ||
         cudaMallocHost(reinterpret_cast<void**>(&c->host_u64), 4 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
@@ -411,7 +413,7 @@ void grt_destroy(grt_ctx* c) {
     c->image.release(); c->spectrum.release(); c->arrived.release(); c->scratch_u64.release();
     c->images_dev.release(); c->image_start_dev.release();
     c->group_qstart_dev.release(); c->group_chan_dev.release(); c->chan_img_dev.release();
-    c->order_ph.release(); c->order_geo.release();
+    c->order_ph.release(); c->order_geo.release(); c->sm_claims.release();
     c->m_abs.release(); c->m_emis.release();
     c->ckpt.release(); c->tape.release(); c->dLdI.release(); c->g_abs.release(); c->g_emis.release();
     c->nckpt.release(); c->adj_overflow.release(); c->call0.release();
@@ -1048,8 +1050,22 @@ int trace_blocks_per_sm(const grt_ctx* c, unsigned long long queue) {
     return 4;
 }
 
-cudaError_t launch_trace(const grt_ctx* c, const grt::KParams& kp, size_t smem) {
-    const int bps = trace_blocks_per_sm(c, kp.n);
+// When every queue claim of a launch fits in its resident warps (C1, C2: no
+// warp ever refills from the queue), the first claims are balanced over the
+// SMs: at most ceil(claims / SMs) per SM (KParams::sm_quota).  Each launch
+// zeroes the counters first, as a node of the render graph too.
+cudaError_t launch_trace(const grt_ctx* c, const grt::KParams& kp_in, size_t smem) {
+    const int bps = trace_blocks_per_sm(c, kp_in.n);
+    grt::KParams kp = kp_in;
+    const unsigned long long warps = static_cast<unsigned long long>(c->sm_count) * bps * 4;
+    const unsigned long long claims = kp.grab > 0 ? (kp.n + kp.grab - 1) / kp.grab : 0;
+    if (c->sm_claims.ptr && claims > 0 && claims <= warps) {
+        kp.sm_claims = c->sm_claims.ptr;
+        kp.sm_quota = static_cast<unsigned>((claims + c->sm_count - 1) / c->sm_count);
+        const cudaError_t e0 =
+            cudaMemsetAsync(kp.sm_claims, 0, grt::kSmClaimSlots * sizeof(unsigned), c->stream);
+        if (e0 != cudaSuccess) return e0;
+    }
     const grt_params& p = c->p;
     const bool mixed = p.precision != GRT_PREC_FP64;
     if (!split_legs(c)) {
@@ -1065,6 +1081,8 @@ cudaError_t launch_trace(const grt_ctx* c, const grt::KParams& kp, size_t smem) 
             kp, c->sm_count,
             grt::dev_trace_smem_bytes(0, 128, c->fluid_available && c->separable, c->nr, c->nth, c->nph), c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(&kp.counters->queue_head, 0, sizeof(unsigned long long), c->stream);
+    if (e == cudaSuccess && kp.sm_quota)
+        e = cudaMemsetAsync(kp.sm_claims, 0, grt::kSmClaimSlots * sizeof(unsigned), c->stream);
     if (e == cudaSuccess)
         e = grt::launch_trace(kp, mixed, 2, p.integrator, c->sm_count, bps, smem, c->stream);
     return e;

@@ -56,6 +56,9 @@ struct KPhotons {
 };
 
 // Counters one trace launch accumulates (all zeroed before the launch).
+// Per-SM first-claim counters (KParams::sm_claims), indexed by %smid.
+constexpr unsigned kSmClaimSlots = 1024;
+
 struct KCounters {
     unsigned long long queue_head;        // next photon index to hand out
     unsigned long long terminated;        // photons that terminated in this launch
@@ -120,6 +123,12 @@ struct KParams {
     // geodesic as the last launch left it; zeroed with the photons' init
     // (nullptr: channel 0 leads and none finished)
     unsigned long long* share_state;
+    // first-fill balance: when every queue claim fits in the resident warps,
+    // a warp's first claim is allowed only while its SM (%smid) has taken
+    // fewer than sm_quota first claims (sm_claims: kSmClaimSlots counters,
+    // zeroed before each launch); 0 = off
+    unsigned* sm_claims;
+    unsigned sm_quota;
     // image mode: queue position -> queue index, so that each warp's 32
     // claims are an 8 x 4 tile of one image's pixels (nullptr = identity)
     const unsigned* order;
