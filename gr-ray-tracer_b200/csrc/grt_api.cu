@@ -383,7 +383,8 @@ grt_status grt_create(const grt_params* p, grt_ctx** out) {
     c->device = dev;
     c->sm_count = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        c->counters.alloc(1) != cudaSuccess || c->sm_claims.alloc(grt::kSmClaimSlots) != cudaSuccess || c->scratch_u64.alloc(4) != cudaSuccess ||
+        c->counters.alloc(1) != cudaSuccess || c->sm_claims.alloc(grt::kSmClaimSlots) != cudaSuccess ||
+        c->scratch_u64.alloc(4) != cudaSuccess ||
         cudaMallocHost(reinterpret_cast<void**>(&c->host_counters), sizeof(grt::KCounters)) != cudaSuccess ||
         cudaMallocHost(reinterpret_cast<void**>(&c->host_u64), 4 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
