@@ -164,7 +164,10 @@ typedef struct grt_launch_config {
     int32_t blocks_per_sm;        /* 2, 3 or 4 resident blocks per SM: register caps 255 / 170 / 128;
                                      0 = automatic: the fewest that keep every geodesic resident */
     int32_t refill_threshold;     /* idle lanes in a warp before it pulls new photons (1..32) */
-    int32_t photons_per_grab;     /* photons a warp claims per access to the global queue */
+    int32_t photons_per_grab;     /* photons a warp claims per access to the global queue; an
+                                     image-mode queue is laid out in 8 x 4 pixel tiles, so 32 is
+                                     one tile.  When every claim fits in the resident warps, the
+                                     first claims are spread evenly over the SMs. */
     int32_t split_legs;           /* image mode: 1 = the backward legs, the packet generation at first
                                      fluid contact and the rest as three launches (same results, smaller
                                      loop bodies); 0 = one launch for whole rays */
