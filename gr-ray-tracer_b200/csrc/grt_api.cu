@@ -177,6 +177,9 @@ struct grt_ctx {
     // tile orders of the image-mode queue (queue position -> index): over
     // photon slots and over the geodesics of channel groups
     DevBuf<unsigned> order_ph, order_geo;
+    // layout the tile orders were built for (image slot starts and widths,
+    // group starts and widths): a new image set with the same layout reuses them
+    std::vector<unsigned long long> order_layout;
     // per-SM first-claim counters of the trace launches (KParams::sm_claims)
     DevBuf<unsigned> sm_claims;
     bool order_ph_ok = false, order_geo_ok = false;
@@ -804,8 +807,17 @@ void append_tile_order(std::vector<unsigned>& out, unsigned long long start, uin
 grt_status set_tile_orders(grt_ctx* c, const std::vector<unsigned long long>& start,
                            const std::vector<unsigned long long>& qstart, const std::vector<int>& gchan,
                            const std::vector<int>& chan) {
+    std::vector<unsigned long long> layout(start.begin(), start.end());
+    for (const grt_image_spec& sp : c->images) layout.push_back(sp.nx);
+    layout.push_back(~0ull);
+    layout.insert(layout.end(), qstart.begin(), qstart.end());
+    for (size_t g = 0; g + 1 < qstart.size(); ++g) layout.push_back(c->images[chan[gchan[g]]].nx);
+    const bool usable = !c->random_screen && c->n < (1ull << 32);
+    if (usable && layout == c->order_layout && c->order_ph_ok && (qstart.empty() || c->order_geo_ok))
+        return GRT_OK;  // same layout: the orders on the device still hold
     c->order_ph_ok = c->order_geo_ok = false;
-    if (c->random_screen || c->n >= (1ull << 32)) return GRT_OK;
+    c->order_layout.clear();
+    if (!usable) return GRT_OK;
     std::vector<unsigned> ord;
     ord.reserve(c->n);
     for (size_t k = 0; k + 1 < start.size(); ++k)
@@ -825,6 +837,7 @@ grt_status set_tile_orders(grt_ctx* c, const std::vector<unsigned long long>& st
                  "H2D queue order");
         c->order_geo_ok = ord.size() == c->geodesics;
     }
+    c->order_layout = std::move(layout);
     return GRT_OK;
 }
 

@@ -71,3 +71,36 @@ def test_cut_tiles_of_a_channel_group(gpu):
         for f in abi.PHOTON_FIELDS:
             assert np.array_equal(getattr(batch, f)[start:start + 91], getattr(single, f)), f
         start += 91
+
+
+def test_reinitialised_layouts_match_fresh_contexts(gpu):
+    # one context through three image sets: a batch, a single odd screen, the
+    # batch again (the tile orders are rebuilt, then reused for the same
+    # layout); each run must equal the same image set on a fresh context
+    p = screen_params(C2_SMALL, 13, 7)
+    grid = C2_SMALL.torus()
+    specs = [abi.ImageSpec.from_params(p, 16, 12, camera_theta=math.radians(30.0)),
+             abi.ImageSpec.from_params(p, 9, 5, camera_theta=math.radians(60.0), custom_frequency_hz=86e9)]
+
+    def fresh(kind):
+        c = gpu.Context(p)
+        try:
+            c.upload_grid(grid)
+            c.init_image_batch(specs) if kind == "batch" else c.init_image_photons(13, 7)
+            c.run()
+            return c.download_photons()
+        finally:
+            c.close()
+
+    want = {kind: fresh(kind) for kind in ("batch", "single")}
+    ctx = gpu.Context(p)
+    try:
+        ctx.upload_grid(grid)
+        for kind in ("batch", "single", "batch"):
+            ctx.init_image_batch(specs) if kind == "batch" else ctx.init_image_photons(13, 7)
+            ctx.run()
+            got = ctx.download_photons()
+            for f in abi.PHOTON_FIELDS:
+                assert np.array_equal(getattr(got, f), getattr(want[kind], f)), (kind, f)
+    finally:
+        ctx.close()
